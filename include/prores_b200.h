@@ -1,0 +1,206 @@
+/*
+ * prores_b200.h -- C ABI of the B200 ProRes (SMPTE RDD 36) slice pipeline.
+ *
+ * The entry points replace the rivet-prores crate's public codec API
+ * (imported as `prores`): Decoder::{new, with_bit_depth, with_threads,
+ * decode} (src/decode.rs:28-104), Encoder::{new, encode} with Config and
+ * Profile (src/encode.rs:31-287), and the Error kinds (src/error.rs:6-21).
+ * Plain pointers and sizes only; no CUDA or torch types cross this boundary.
+ *
+ * Frame layout (src/frame.rs:172-266): one u16 buffer holding Y', then Cb,
+ * then Cr, each tightly packed (stride == width); 4:2:2 chroma planes are
+ * ceil(width/2) wide. Alpha, when present, is a separate width*height plane.
+ * Samples carry their value in the low bit_depth bits.
+ *
+ * Threading: a context may be used from several threads at once; each call
+ * takes its own device workspace and stream. Output never depends on the
+ * batch composition, the thread count or the launch shape.
+ */
+#ifndef PRORES_B200_H
+#define PRORES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. 1-3 are the crate's Error::{Invalid, Unsupported, Config}
+ * (src/error.rs:6-21) and come back for exactly the inputs the crate refuses;
+ * 4 and 5 are new: a CUDA failure, and a device wait that ran out. */
+#define PRORES_OK 0
+#define PRORES_INVALID 1
+#define PRORES_UNSUPPORTED 2
+#define PRORES_CONFIG 3
+#define PRORES_DEVICE 4
+#define PRORES_TIMEOUT 5
+
+/* chroma_format codes (src/frame.rs:25-40) */
+#define PRORES_CHROMA_422 2
+#define PRORES_CHROMA_444 3
+
+/* Profile (src/encode.rs:30-44), lowest rate first. */
+#define PRORES_PROFILE_PROXY 0
+#define PRORES_PROFILE_LT 1
+#define PRORES_PROFILE_STANDARD 2
+#define PRORES_PROFILE_HQ 3
+#define PRORES_PROFILE_4444 4
+#define PRORES_PROFILE_4444XQ 5
+
+/* alpha_channel_type (src/header.rs:10-40) */
+#define PRORES_ALPHA_NONE 0
+#define PRORES_ALPHA_8 1
+#define PRORES_ALPHA_16 2
+
+typedef struct prores_ctx prores_ctx;
+
+/* A picture (src/frame.rs:179-203). For decode into caller memory, set
+ * data/alpha to buffers of data_len/alpha_len samples (prores_probe gives
+ * the sizes); with data == NULL the library allocates and
+ * prores_frame_free releases. */
+typedef struct prores_frame {
+    uint32_t width, height, bit_depth;
+    int32_t chroma;    /* PRORES_CHROMA_422 or PRORES_CHROMA_444 */
+    int32_t interlace; /* 0 progressive, 1 top field first, 2 bottom field first */
+    uint8_t aspect_ratio, frame_rate_code, color_primaries, transfer_characteristic,
+        matrix_coefficients, reserved_[3]; /* Metadata (src/frame.rs:84-96) */
+    uint16_t *data;
+    size_t data_len; /* samples in data */
+    uint16_t *alpha; /* NULL: no alpha plane */
+    size_t alpha_len;
+} prores_frame;
+
+/* Config (src/encode.rs:135-174). Defaults (Config::new): log2_slice_mbs 3,
+ * alpha PRORES_ALPHA_16, no matrices, target_frame_bytes -1 (the profile's),
+ * encoder_identifier "rivt", threads 0. prores_config_default fills them. */
+typedef struct prores_config {
+    int32_t profile;
+    uint32_t log2_slice_mbs;
+    int32_t alpha;
+    int32_t has_luma_matrix, has_chroma_matrix;
+    uint8_t luma_matrix[64], chroma_matrix[64]; /* raster order, weights 2-63 */
+    int64_t target_frame_bytes;                 /* < 0: Profile::target_frame_bytes */
+    uint8_t encoder_identifier[4];
+    uint32_t threads; /* accepted and ignored: the output does not depend on it */
+} prores_config;
+
+/* One byte buffer (a ProRes frame: the bytes of one MOV sample). */
+typedef struct prores_buf {
+    const uint8_t *data;
+    size_t len;
+} prores_buf;
+
+/* The parsed frame header (FrameHeader, src/header.rs:43-72). */
+typedef struct prores_frame_header {
+    uint32_t frame_size;
+    uint16_t header_size;
+    uint8_t bitstream_version;
+    uint8_t encoder_identifier[4];
+    uint8_t reserved_;
+    uint16_t width, height;
+    int32_t chroma, interlace, alpha; /* alpha: PRORES_ALPHA_* */
+    uint8_t aspect_ratio, frame_rate_code, color_primaries, transfer_characteristic,
+        matrix_coefficients, reserved2_[3];
+    int32_t has_luma_matrix, has_chroma_matrix;
+    uint8_t luma_matrix[64], chroma_matrix[64]; /* raster order */
+} prores_frame_header;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* A context on CUDA device `device`; NULL on failure (no device, or not
+ * sm_100). Replaces constructing Decoder/Encoder values: the crate's are
+ * stateless settings holders, this one owns device workspaces. */
+prores_ctx *prores_create(int device);
+void prores_destroy(prores_ctx *ctx);
+
+/* Message of the last failing call made on this thread, formatted like the
+ * crate's Error Display ("invalid ProRes data: ..."). */
+const char *prores_last_error(void);
+
+/* Message of frame i of the last batch call (decode or encode, including a
+ * job's fetch) made on this thread; "" when that frame succeeded. */
+const char *prores_batch_error(int i);
+
+/* ---- decode (Decoder::decode, src/decode.rs:61-104) ------------------- */
+
+/* Parses the frame header (FrameHeader::parse, src/header.rs:82-170) and the
+ * plausibility check (src/decode.rs:113-128) without decoding: fills
+ * width/height/bit_depth/chroma/interlace/metadata, data_len and alpha_len.
+ * out_bit_depth 0 is the natural depth (10 for 4:2:2, 12 for 4:4:4); else
+ * 8-16 (Decoder::with_bit_depth, src/decode.rs:37-47). */
+int prores_probe(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info);
+
+/* FrameHeader::parse (src/header.rs:82-170): host only, no device needed. */
+int prores_parse_frame_header(const uint8_t *data, size_t len, prores_frame_header *out);
+
+/* Decodes one frame. Bytes after frame_size are ignored. */
+int prores_decode(prores_ctx *ctx, const uint8_t *data, size_t len, uint32_t out_bit_depth,
+                  prores_frame *out);
+
+/* Decodes n frames of any sizes and formats in one batched launch. status[i]
+ * gets each frame's code (the message of the first failing one is kept for
+ * prores_last_error); the call returns PRORES_OK unless a device error hit
+ * the whole batch. */
+int prores_decode_batch(prores_ctx *ctx, const prores_buf *in, int n, uint32_t out_bit_depth,
+                        prores_frame *out, int *status);
+
+void prores_frame_free(prores_frame *f);
+
+/* ---- encode (Encoder::encode, src/encode.rs:223-287) ------------------ */
+
+void prores_config_default(prores_config *cfg, int32_t profile);
+
+/* Profile::target_frame_bytes (src/encode.rs:112-117). */
+size_t prores_target_frame_bytes(int32_t profile, uint32_t width, uint32_t height);
+
+/* Encodes one frame into a library-allocated packet (prores_buffer_free). */
+int prores_encode(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, uint8_t **out,
+                  size_t *out_len);
+
+/* Encodes n frames (each with its own config) in one batched launch; out[i]
+ * gets a library-allocated packet (prores_buffer_free each data). */
+int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n,
+                        prores_buf *out, int *status);
+
+void prores_buffer_free(void *p);
+
+/* ---- resident jobs (batching and serving) ----------------------------- */
+
+/* A decode job keeps a batch's bitstreams and planes resident in device
+ * memory so that the batch can be decoded again without host traffic (and,
+ * with use_graph, as one CUDA-graph launch). `stream` is a cudaStream_t
+ * given as void* (NULL: the job's own stream). */
+typedef struct prores_decode_job prores_decode_job;
+int prores_decode_job_create(prores_ctx *ctx, const prores_buf *in, int n, uint32_t out_bit_depth,
+                             prores_decode_job **job);
+/* Enqueues the device work only (kernels over the resident bitstreams into
+ * the resident planes); returns without waiting. */
+int prores_decode_job_launch(prores_decode_job *job, void *stream, int use_graph);
+/* Copies new bitstreams of the same sizes in (host to device) on `stream`. */
+int prores_decode_job_upload(prores_decode_job *job, const prores_buf *in, int n, void *stream);
+/* Waits for `stream`, copies the planes out and sets status[i]. */
+int prores_decode_job_fetch(prores_decode_job *job, void *stream, prores_frame *out, int *status);
+/* Device pointer of frame i's planes (Y'‖Cb‖Cr) and alpha in the job. */
+int prores_decode_job_planes(prores_decode_job *job, int i, uint16_t **data, uint16_t **alpha);
+void prores_decode_job_destroy(prores_decode_job *job);
+
+typedef struct prores_encode_job prores_encode_job;
+int prores_encode_job_create(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n,
+                             prores_encode_job **job);
+int prores_encode_job_launch(prores_encode_job *job, void *stream, int use_graph);
+int prores_encode_job_upload(prores_encode_job *job, const prores_frame *in, int n, void *stream);
+/* Waits for `stream`; out[i].data points into job-owned host memory valid
+ * until the next fetch or destroy. */
+int prores_encode_job_fetch(prores_encode_job *job, void *stream, prores_buf *out, int *status);
+void prores_encode_job_destroy(prores_encode_job *job);
+
+/* Per-kernel device time of the last launch of a job that was created with
+ * profiling on (PRORES_PROFILE_KERNELS=1 in the environment): names[i] and
+ * ms[i] for up to cap kernels; returns the count. */
+int prores_job_kernel_times(const void *job, int is_encode, const char **names, float *ms, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

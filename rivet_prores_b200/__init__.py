@@ -1,0 +1,518 @@
+"""B200-native ProRes (SMPTE RDD 36) decode and encode.
+
+A drop-in for the rivet-prores crate's public API (imported there as
+`prores`, src/lib.rs:52-56): `Decoder`, `Encoder`, `Config`, `Profile`,
+`Frame`, `Plane`, `ChromaFormat`, `Interlace`, `Metadata`, `FrameHeader`,
+`AlphaType`, `Error`. Every per-slice step runs in the sm_100a kernels of
+libprores_b200.so; decoded planes and encoded bytes are bit-identical to the
+crate's. Batched forms (`Decoder.decode_batch`, `Encoder.encode_batch`) put
+many frames of any size and format into one launch.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+import threading
+from dataclasses import dataclass, field, replace
+from typing import List, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _abi
+from ._abi import Buf_, Config_, Frame_, FrameHeader_
+
+__all__ = [
+    "AlphaType", "ChromaFormat", "Config", "Decoder", "Encoder", "Error", "Frame", "FrameHeader",
+    "Interlace", "Metadata", "Plane", "Profile", "context",
+]
+
+
+# ------------------------------------------------------------------ errors
+
+class Error(Exception):
+    """src/error.rs:6-21: Invalid, Unsupported and Config, each with a message;
+    Device and Timeout are this library's (a CUDA failure, a wait that ran out).
+    Catch a kind as `Error.Invalid`, `Error.Unsupported`, `Error.Config`."""
+
+    kind = "Error"
+
+    def __init__(self, message: str):
+        super().__init__(message)
+        self.message = message
+
+    def __eq__(self, other):
+        return type(self) is type(other) and self.message == other.message
+
+    def __hash__(self):
+        return hash((type(self).__name__, self.message))
+
+
+class _Invalid(Error):
+    kind = "Invalid"
+
+
+class _Unsupported(Error):
+    kind = "Unsupported"
+
+
+class _Config(Error):
+    kind = "Config"
+
+
+class _Device(Error):
+    kind = "Device"
+
+
+class _Timeout(Error):
+    kind = "Timeout"
+
+
+Error.Invalid = _Invalid
+Error.Unsupported = _Unsupported
+Error.Config = _Config
+Error.Device = _Device
+Error.Timeout = _Timeout
+_KINDS = {_abi.INVALID: _Invalid, _abi.UNSUPPORTED: _Unsupported, _abi.CONFIG: _Config,
+          _abi.DEVICE: _Device, _abi.TIMEOUT: _Timeout}
+
+
+def _error(code: int, message: Optional[str] = None) -> Error:
+    return _KINDS.get(code, _Device)(message if message is not None else _abi.last_error())
+
+
+def _check(code: int):
+    if code != _abi.OK:
+        raise _error(code)
+
+
+# ------------------------------------------------------------------ types
+
+class ChromaFormat(enum.Enum):
+    """src/frame.rs:8-41."""
+
+    Yuv422 = 2
+    Yuv444 = 3
+
+    def subsampling(self):
+        return (2, 1) if self is ChromaFormat.Yuv422 else (1, 1)
+
+    def code(self) -> int:
+        return self.value
+
+    @staticmethod
+    def from_code(code: int) -> Optional["ChromaFormat"]:
+        return {2: ChromaFormat.Yuv422, 3: ChromaFormat.Yuv444}.get(code)
+
+
+class Interlace(enum.Enum):
+    """src/frame.rs:47-77: woven output, the top field on the even rows."""
+
+    Progressive = 0
+    TopFieldFirst = 1
+    BottomFieldFirst = 2
+
+    def code(self) -> int:
+        return self.value
+
+    @staticmethod
+    def from_code(code: int) -> Optional["Interlace"]:
+        return {0: Interlace.Progressive, 1: Interlace.TopFieldFirst, 2: Interlace.BottomFieldFirst}.get(code)
+
+
+class AlphaType(enum.Enum):
+    """src/header.rs:10-40."""
+
+    None_ = 0
+    Bits8 = 1
+    Bits16 = 2
+
+    def code(self) -> int:
+        return self.value
+
+    def bits(self) -> int:
+        return {0: 0, 1: 8, 2: 16}[self.value]
+
+
+_FRAME_RATES = {1: (24000, 1001), 2: (24, 1), 3: (25, 1), 4: (30000, 1001), 5: (30, 1), 6: (50, 1),
+                7: (60000, 1001), 8: (60, 1), 9: (100, 1), 10: (120000, 1001), 11: (120, 1)}
+
+
+@dataclass(frozen=True)
+class Metadata:
+    """src/frame.rs:83-146: the frame header's descriptive codes."""
+
+    aspect_ratio: int = 0
+    frame_rate_code: int = 0
+    color_primaries: int = 2
+    transfer_characteristic: int = 2
+    matrix_coefficients: int = 2
+
+    def frame_rate(self):
+        return _FRAME_RATES.get(self.frame_rate_code)
+
+    @staticmethod
+    def frame_rate_code_for(numerator: int, denominator: int) -> int:
+        for c, (n, d) in _FRAME_RATES.items():
+            if n * denominator == numerator * d:
+                return c
+        return 0
+
+
+@dataclass(frozen=True)
+class Plane:
+    """src/frame.rs:148-170: where a plane sits in `Frame.data` (samples)."""
+
+    offset: int
+    width: int
+    height: int
+
+    def len(self) -> int:
+        return self.width * self.height
+
+    def is_empty(self) -> bool:
+        return self.len() == 0
+
+
+def _layout(width: int, height: int, chroma: ChromaFormat) -> List[Plane]:
+    cw = -(-width // chroma.subsampling()[0])
+    y = Plane(0, width, height)
+    cb = Plane(y.len(), cw, height)
+    cr = Plane(cb.offset + cb.len(), cw, height)
+    return [y, cb, cr]
+
+
+@dataclass
+class Frame:
+    """src/frame.rs:179-341: packed u16 planes Y', Cb, Cr and an optional alpha
+    plane, values in the low `bit_depth` bits."""
+
+    width: int
+    height: int
+    bit_depth: int
+    chroma: ChromaFormat
+    interlace: Interlace = Interlace.Progressive
+    metadata: Metadata = field(default_factory=Metadata)
+    data: np.ndarray = None
+    planes: List[Plane] = None
+    alpha: Optional[np.ndarray] = None
+
+    @staticmethod
+    def new(width: int, height: int, chroma: ChromaFormat, bit_depth: int) -> "Frame":
+        """Mid-grey, no alpha, progressive (src/frame.rs:209-245)."""
+        if width == 0 or height == 0 or width > 65535 or height > 65535:
+            raise Error.Config(f"invalid ProRes configuration: a frame of {width}×{height} cannot be coded "
+                               "(1–65535 each way)")
+        if not 8 <= bit_depth <= 16:
+            raise Error.Config(f"invalid ProRes configuration: bit depth {bit_depth} is outside 8–16")
+        planes = _layout(width, height, chroma)
+        total = planes[2].offset + planes[2].len()
+        return Frame(width, height, bit_depth, chroma, Interlace.Progressive, Metadata(),
+                     np.full(total, 1 << (bit_depth - 1), np.uint16), planes, None)
+
+    def plane(self, i: int) -> np.ndarray:
+        p = self.planes[i]
+        return self.data[p.offset:p.offset + p.len()]
+
+    plane_mut = plane
+
+    def plane2d(self, i: int) -> np.ndarray:
+        p = self.planes[i]
+        return self.plane(i).reshape(p.height, p.width)
+
+    def packed(self) -> np.ndarray:
+        return self.data
+
+    def to_le_bytes(self) -> bytes:
+        return self.data.astype("<u2").tobytes()
+
+
+@dataclass
+class FrameHeader:
+    """src/header.rs:43-255: the parsed frame header."""
+
+    frame_size: int
+    header_size: int
+    bitstream_version: int
+    encoder_identifier: bytes
+    width: int
+    height: int
+    chroma: ChromaFormat
+    interlace: Interlace
+    metadata: Metadata
+    alpha: AlphaType
+    luma_matrix: Optional[bytes]
+    chroma_matrix: Optional[bytes]
+
+    @staticmethod
+    def parse(data: bytes) -> "FrameHeader":
+        h = FrameHeader_()
+        data = bytes(data)
+        _check(_abi.lib().prores_parse_frame_header(data, len(data), ctypes.byref(h)))
+        return FrameHeader(
+            h.frame_size, h.header_size, h.bitstream_version, bytes(h.encoder_identifier), h.width, h.height,
+            ChromaFormat(h.chroma), Interlace(h.interlace),
+            Metadata(h.aspect_ratio, h.frame_rate_code, h.color_primaries, h.transfer_characteristic,
+                     h.matrix_coefficients),
+            AlphaType(h.alpha), bytes(h.luma_matrix) if h.has_luma_matrix else None,
+            bytes(h.chroma_matrix) if h.has_chroma_matrix else None)
+
+    def picture_count(self) -> int:
+        return 1 if self.interlace is Interlace.Progressive else 2
+
+    def _is_top(self, index: int) -> bool:
+        return (self.interlace is Interlace.TopFieldFirst) == (index == 0)
+
+    def picture_height(self, index: int) -> int:
+        if self.interlace is Interlace.Progressive:
+            return self.height
+        return (self.height + 1) // 2 if self._is_top(index) else self.height // 2
+
+
+# ------------------------------------------------------------------ profiles
+
+class Profile(enum.Enum):
+    """src/encode.rs:26-118."""
+
+    Proxy = 0
+    Lt = 1
+    Standard = 2
+    Hq = 3
+    P4444 = 4
+    P4444Xq = 5
+
+    def fourcc(self) -> bytes:
+        return [b"apco", b"apcs", b"apcn", b"apch", b"ap4h", b"ap4x"][self.value]
+
+    @staticmethod
+    def from_fourcc(code: bytes) -> Optional["Profile"]:
+        for p in Profile:
+            if p.fourcc() == bytes(code):
+                return p
+        return None
+
+    def chroma(self) -> ChromaFormat:
+        return ChromaFormat.Yuv444 if self.value >= 4 else ChromaFormat.Yuv422
+
+    def reference_bitrate(self) -> int:
+        return [45_000_000, 102_000_000, 147_000_000, 220_000_000, 330_000_000, 500_000_000][self.value]
+
+    def target_frame_bytes(self, width: int, height: int) -> int:
+        return int(_abi.lib().prores_target_frame_bytes(self.value, width, height))
+
+
+Profile.ALL = [Profile.Proxy, Profile.Lt, Profile.Standard, Profile.Hq, Profile.P4444, Profile.P4444Xq]
+
+
+@dataclass
+class Config:
+    """src/encode.rs:133-193."""
+
+    profile: Profile
+    log2_slice_mbs: int = 3
+    alpha: AlphaType = AlphaType.Bits16
+    luma_matrix: Optional[bytes] = None
+    chroma_matrix: Optional[bytes] = None
+    target_frame_bytes: Optional[int] = None
+    encoder_identifier: bytes = b"rivt"
+    threads: int = 0
+
+    @staticmethod
+    def new(profile: Profile) -> "Config":
+        return Config(profile)
+
+    def _c(self) -> Config_:
+        c = Config_()
+        c.profile = self.profile.value
+        c.log2_slice_mbs = self.log2_slice_mbs
+        c.alpha = self.alpha.value
+        if self.luma_matrix is not None:
+            c.has_luma_matrix = 1
+            c.luma_matrix[:] = list(bytes(self.luma_matrix))
+        if self.chroma_matrix is not None:
+            c.has_chroma_matrix = 1
+            c.chroma_matrix[:] = list(bytes(self.chroma_matrix))
+        c.target_frame_bytes = -1 if self.target_frame_bytes is None else int(self.target_frame_bytes)
+        c.encoder_identifier[:] = list(bytes(self.encoder_identifier)[:4])
+        c.threads = self.threads
+        return c
+
+
+# ------------------------------------------------------------------ device
+
+class Context:
+    """A device context (workspaces and streams) of libprores_b200."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.handle = _abi.lib().prores_create(device)
+        if not self.handle:
+            raise Error.Device(_abi.last_error())
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        lib = getattr(_abi, "_lib", None) if _abi is not None else None
+        if h and lib is not None:
+            lib.prores_destroy(h)
+            self.handle = None
+
+
+_contexts = {}
+_ctx_lock = threading.Lock()
+
+
+def context(device: int = 0) -> Context:
+    """The process-wide context of `device` (created on first use)."""
+    with _ctx_lock:
+        if device not in _contexts:
+            _contexts[device] = Context(device)
+        return _contexts[device]
+
+
+def _frame_from_c(f: Frame_, data: np.ndarray, alpha: Optional[np.ndarray]) -> Frame:
+    chroma = ChromaFormat(f.chroma)
+    return Frame(f.width, f.height, f.bit_depth, chroma, Interlace(f.interlace),
+                 Metadata(f.aspect_ratio, f.frame_rate_code, f.color_primaries, f.transfer_characteristic,
+                          f.matrix_coefficients),
+                 data, _layout(f.width, f.height, chroma), alpha)
+
+
+def _ptr16(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
+
+
+class Decoder:
+    """src/decode.rs:15-104. Stateless settings; decoding runs on the GPU."""
+
+    def __init__(self, bit_depth: Optional[int] = None, threads: int = 0, device: int = 0):
+        self.bit_depth = bit_depth
+        self.threads = threads
+        self.device = device
+
+    @staticmethod
+    def new() -> "Decoder":
+        return Decoder()
+
+    @staticmethod
+    def with_bit_depth(bit_depth: int) -> "Decoder":
+        if not 8 <= bit_depth <= 16:
+            raise Error.Config(f"invalid ProRes configuration: output bit depth {bit_depth} is outside 8–16")
+        return Decoder(bit_depth)
+
+    def with_threads(self, threads: int) -> "Decoder":
+        """Accepted for the crate's API; the output does not depend on it."""
+        return replace_decoder(self, threads=threads)
+
+    def decode(self, data: bytes) -> Frame:
+        r = self.decode_batch([data])[0]
+        if isinstance(r, Error):
+            raise r
+        return r
+
+    def decode_batch(self, datas: Sequence[bytes]) -> List[Union[Frame, Error]]:
+        """Decodes every frame in one batched launch; each entry is a Frame or
+        the Error that frame gave."""
+        L = _abi.lib()
+        n = len(datas)
+        datas = [bytes(d) for d in datas]
+        depth = self.bit_depth or 0
+        bufs = (Buf_ * max(n, 1))()
+        outs = (Frame_ * max(n, 1))()
+        status = (ctypes.c_int * max(n, 1))()
+        results: List[Union[Frame, Error, None]] = [None] * n
+        arrays = [None] * n
+        keep = []
+        for i, d in enumerate(datas):
+            arr = (ctypes.c_uint8 * max(len(d), 1)).from_buffer_copy(d if d else b"\0")
+            keep.append(arr)
+            bufs[i].data = ctypes.cast(arr, ctypes.POINTER(ctypes.c_uint8))
+            bufs[i].len = len(d)
+            info = Frame_()
+            if L.prores_probe(d, len(d), depth, ctypes.byref(info)) == _abi.OK:
+                data = np.empty(info.data_len, np.uint16)
+                alpha = np.empty(info.alpha_len, np.uint16) if info.alpha_len else None
+                outs[i].data, outs[i].data_len = _ptr16(data), info.data_len
+                if alpha is not None:
+                    outs[i].alpha, outs[i].alpha_len = _ptr16(alpha), info.alpha_len
+                arrays[i] = (data, alpha)
+        code = L.prores_decode_batch(context(self.device).handle, bufs, n, depth, outs, status)
+        if code != _abi.OK:
+            raise _error(code)
+        for i in range(n):
+            if status[i] != _abi.OK:
+                results[i] = _error(status[i], _abi.batch_error(i))
+            else:
+                data, alpha = arrays[i]
+                results[i] = _frame_from_c(outs[i], data, alpha)
+        return results
+
+
+def replace_decoder(d: Decoder, **kw) -> Decoder:
+    return Decoder(kw.get("bit_depth", d.bit_depth), kw.get("threads", d.threads), kw.get("device", d.device))
+
+
+def _frame_to_c(f: Frame, keep: list) -> Frame_:
+    c = Frame_()
+    c.width, c.height, c.bit_depth = f.width, f.height, f.bit_depth
+    c.chroma = f.chroma.value
+    c.interlace = f.interlace.value
+    m = f.metadata
+    (c.aspect_ratio, c.frame_rate_code, c.color_primaries, c.transfer_characteristic,
+     c.matrix_coefficients) = (m.aspect_ratio, m.frame_rate_code, m.color_primaries, m.transfer_characteristic,
+                               m.matrix_coefficients)
+    d = np.ascontiguousarray(f.data, dtype=np.uint16)
+    keep.append(d)
+    c.data, c.data_len = _ptr16(d), d.size
+    if f.alpha is not None:
+        a = np.ascontiguousarray(f.alpha, dtype=np.uint16)
+        keep.append(a)
+        c.alpha, c.alpha_len = _ptr16(a), a.size
+    return c
+
+
+class Encoder:
+    """src/encode.rs:195-287."""
+
+    def __init__(self, config: Config, device: int = 0):
+        self._config = config
+        self.device = device
+
+    @staticmethod
+    def new(config: Config) -> "Encoder":
+        return Encoder(config)
+
+    def config(self) -> Config:
+        return self._config
+
+    def encode(self, frame: Frame) -> bytes:
+        r = self.encode_batch([frame])[0]
+        if isinstance(r, Error):
+            raise r
+        return r
+
+    def encode_batch(self, frames: Sequence[Frame], configs: Optional[Sequence[Config]] = None
+                     ) -> List[Union[bytes, Error]]:
+        """Encodes every frame (each with its own Config, default this
+        encoder's) in one batched launch."""
+        L = _abi.lib()
+        n = len(frames)
+        configs = list(configs) if configs is not None else [self._config] * n
+        keep = []
+        cfgs = (Config_ * max(n, 1))()
+        ins = (Frame_ * max(n, 1))()
+        outs = (Buf_ * max(n, 1))()
+        status = (ctypes.c_int * max(n, 1))()
+        for i in range(n):
+            cfgs[i] = configs[i]._c()
+            ins[i] = _frame_to_c(frames[i], keep)
+        code = L.prores_encode_batch(context(self.device).handle, cfgs, ins, n, outs, status)
+        if code != _abi.OK:
+            raise _error(code)
+        res: List[Union[bytes, Error]] = []
+        for i in range(n):
+            if status[i] != _abi.OK:
+                res.append(_error(status[i], _abi.batch_error(i)))
+            else:
+                res.append(ctypes.string_at(outs[i].data, outs[i].len))
+                L.prores_buffer_free(outs[i].data)
+        return res

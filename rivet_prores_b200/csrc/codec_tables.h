@@ -1,0 +1,143 @@
+// codec_tables.h -- RDD 36 constants shared by host and device code: the
+// variable-length codebooks (Tables 9-11, §7.1.1.1), the scans (Figures 4
+// and 5) and Table 15's qScale, with the codeword arithmetic the entropy
+// kernels use. The tables must be RDD 36's, so they match the crate's
+// src/vlc.rs:28-68 and src/tables.rs:6-38 entry for entry.
+#pragma once
+
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define PR_HD __host__ __device__ __forceinline__
+#else
+#define PR_HD inline
+#endif
+
+namespace prores {
+
+// A codebook as RICE_EXP_COMBO_CODE(lastRiceQ q, kRice r, kExp e); an
+// exp-Golomb code of order k is the combination (0, k, k + 1) (the note at
+// the end of RDD 36 §7.1.1.1), and `eg` records which form the table names.
+struct Codebook {
+    uint8_t eg, q, r, e;
+};
+
+#define PR_EG(k) Codebook{1, 0, (uint8_t)(k), (uint8_t)((k) + 1)}
+#define PR_CB(q, r, e) Codebook{0, (uint8_t)(q), (uint8_t)(r), (uint8_t)(e)}
+
+static constexpr Codebook kFirstDcBook = PR_EG(5);
+
+// Longest accepted zero prefix and largest accepted symbol: a bound that
+// keeps every read inside a 64-bit window (the crate's src/vlc.rs:19-26).
+static constexpr uint32_t kMaxPrefix = 32;
+static constexpr uint32_t kMaxSymbol = 1u << 30;
+
+// Figure 4 and Figure 5: scan[8 v + u] is the scanned index of the
+// coefficient at row v, column u.
+static constexpr uint8_t kProgressiveScan[64] = {
+    0,  1,  4,  5,  16, 17, 21, 22, 2,  3,  6,  7,  18, 20, 23, 28, 8,  9,  12, 13, 19, 24,
+    27, 29, 10, 11, 14, 15, 25, 26, 30, 31, 32, 33, 37, 38, 45, 46, 53, 54, 34, 36, 39, 44,
+    47, 52, 55, 60, 35, 40, 43, 48, 51, 56, 59, 61, 41, 42, 49, 50, 57, 58, 62, 63};
+static constexpr uint8_t kInterlacedScan[64] = {
+    0,  2,  8,  10, 32, 34, 35, 41, 1,  3,  9,  11, 33, 36, 40, 42, 4,  6,  12, 14, 37, 39,
+    43, 49, 5,  7,  13, 15, 38, 44, 48, 50, 16, 18, 19, 25, 45, 47, 51, 57, 17, 20, 24, 26,
+    46, 52, 56, 58, 21, 23, 27, 30, 53, 55, 59, 62, 22, 28, 29, 31, 54, 60, 61, 63};
+
+// Table 15.
+PR_HD uint32_t qscale(uint32_t q) { return q <= 128 ? q : 128 + 4 * (q - 128); }
+
+PR_HD uint32_t clz64(uint64_t v) {
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__clzll((long long)v);
+#else
+    return v ? (uint32_t)__builtin_clzll(v) : 64u;
+#endif
+}
+PR_HD uint32_t bit_len64(uint64_t v) { return 64u - clz64(v); }
+
+// Length of an exp-Golomb codeword of order k for n: (q zeros) then n + 2^k
+// in q + k + 1 bits, q = floor(log2(n + 2^k)) - k.
+PR_HD uint32_t eg_len(uint64_t n, uint32_t k) { return 2u * bit_len64(n + (1ull << k)) - k - 1u; }
+
+// Length in bits of the codeword for symbol n.
+PR_HD uint32_t cb_len(Codebook cb, uint32_t n32) {
+    uint64_t n = n32;
+    if (cb.eg) return eg_len(n, cb.r);
+    uint64_t threshold = (uint64_t)(cb.q + 1) << cb.r;
+    if (n < threshold) return (uint32_t)(n >> cb.r) + 1u + cb.r;
+    return cb.q + 1u + eg_len(n - threshold, cb.e);
+}
+
+// The codeword for symbol n as its significant bits (the leading zeros are
+// implied by the length): Rice part `1` + r bits, or the exp-Golomb value
+// n - threshold + 2^e after q + 1 zeros.
+PR_HD uint64_t cb_bits(Codebook cb, uint32_t n32) {
+    uint64_t n = n32;
+    uint64_t threshold = (uint64_t)(cb.q + 1) << cb.r;
+    if (n < threshold) return (1ull << cb.r) | (n & ((1ull << cb.r) - 1));
+    return n - threshold + (1ull << cb.e);
+}
+
+// §7.1.1.2: 0, -1, 1, -2, 2, ... -> 0, 1, 2, 3, 4, ...
+PR_HD uint32_t signed_to_symbol(int32_t n) {
+    return n >= 0 ? 2u * (uint32_t)n : 2u * (0u - (uint32_t)n) - 1u;
+}
+PR_HD int32_t symbol_to_signed(uint32_t s) {
+    return (s & 1u) == 0 ? (int32_t)(s >> 1) : -(int32_t)((s + 1u) >> 1);
+}
+
+// Table 9: the DC difference's codebook by |previousDCDiff| (3 and above
+// share the last entry).
+PR_HD Codebook dc_book(int32_t prev_diff) {
+    const uint32_t a = prev_diff < 0 ? 0u - (uint32_t)prev_diff : (uint32_t)prev_diff;
+    if (a == 0) return PR_EG(0);
+    if (a == 1) return PR_EG(1);
+    if (a == 2) return PR_CB(1, 2, 3);
+    return PR_EG(3);
+}
+// Table 10: the run's codebook by previousRun (15 and above share the last).
+PR_HD Codebook run_book(uint32_t prev_run) {
+    if (prev_run <= 1) return PR_CB(2, 0, 1);
+    if (prev_run <= 3) return PR_CB(1, 0, 1);
+    if (prev_run == 4) return PR_EG(0);
+    if (prev_run <= 8) return PR_CB(1, 1, 2);
+    if (prev_run <= 14) return PR_EG(1);
+    return PR_EG(2);
+}
+// Table 11: abs_level_minus_1's codebook by previousLevelSymbol (8 and above
+// share the last).
+PR_HD Codebook level_book(uint32_t prev) {
+    if (prev == 0) return PR_CB(2, 0, 2);
+    if (prev == 1) return PR_CB(1, 0, 1);
+    if (prev == 2) return PR_CB(2, 0, 1);
+    if (prev == 3) return PR_EG(0);
+    if (prev <= 7) return PR_EG(1);
+    return PR_EG(2);
+}
+
+// Prefix tables for the decoder: for each context and every kDecodeBits-bit
+// window prefix, (symbol << 5) | length of the codeword it starts with, or 0
+// when that codeword is longer.
+static constexpr uint32_t kDecodeBits = 9;
+static constexpr uint32_t kDecodeEntries = 1u << kDecodeBits;
+static constexpr uint32_t kRunTableWords = 16 * kDecodeEntries;
+static constexpr uint32_t kLevelTableWords = 9 * kDecodeEntries;
+
+// `books(c)` gives context c's codebook (run_book or level_book).
+template <class Books>
+inline void build_decode_table(Books books, int n_books, uint16_t *out) {
+    for (int c = 0; c < n_books; c++) {
+        uint16_t *row = out + c * kDecodeEntries;
+        for (uint32_t i = 0; i < kDecodeEntries; i++) row[i] = 0;
+        // Every symbol whose codeword fits, written into each prefix it
+        // starts; symbols past 2^kDecodeBits all have longer codewords.
+        for (uint32_t n = 0; n <= kDecodeEntries; n++) {
+            uint32_t len = cb_len(books((uint32_t)c), n);
+            if (len > kDecodeBits) continue;
+            uint32_t first = (uint32_t)cb_bits(books((uint32_t)c), n) << (kDecodeBits - len);
+            for (uint32_t p = 0; p < (1u << (kDecodeBits - len)); p++) row[first + p] = (uint16_t)((n << 5) | len);
+        }
+    }
+}
+
+}  // namespace prores

@@ -1,0 +1,700 @@
+// decode.cu -- the RDD 36 decoding process (§7) as sm_100a kernels.
+//
+//   k_locate   one CTA per picture: the big-endian u16 slice table, scanned
+//              into slice offsets (src/decode.rs:202-221), each slice's
+//              place in the picture (src/header.rs:308-320), and the first
+//              slice that runs past picture_size.
+//   k_entropy  persistent; one lane per slice component (Y', Cb, Cr, alpha):
+//              the slice header (src/decode.rs:301-338), then the DC and
+//              run/level/sign codes of the interleaved scan (:484-540) into
+//              the coefficient scratch, or the alpha run/difference codes
+//              (:570-595) straight into the alpha plane.
+//   k_idct     one CTA per slice: inverse quantisation, the 8x8 IDCT in the
+//              crate's exact single-precision order (src/dct.rs:36-66,
+//              src/dsp/scalar.rs:8-12) and the sample conversion, stored as
+//              woven 16-byte rows (src/decode.rs:395-438); zeroes the
+//              scratch it read.
+//   k_status   one CTA per picture: the first failing slice component.
+//
+// The f32 arithmetic uses __fmul_rn/__fadd_rn so that nothing is contracted
+// into an FMA: the decoded samples are bit-identical to the crate's.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "codec_tables.h"
+#include "device_types.h"
+
+namespace prores {
+
+__constant__ uint8_t c_scan[2][64];
+
+namespace {
+
+__device__ __forceinline__ uint64_t bswap64(uint64_t v) {
+    uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+    return ((uint64_t)__byte_perm(lo, 0, 0x0123) << 32) | __byte_perm(hi, 0, 0x0123);
+}
+
+__device__ __forceinline__ uint32_t be16(const uint8_t *p) { return ((uint32_t)p[0] << 8) | p[1]; }
+
+// MSB-first reader over [start, end) bits of the bitstream buffer: a pair of
+// aligned 64-bit words funnel-shifted to the position; bits past `end` read
+// as zero (the crate's BitReader::peek64, src/bits.rs:30-40). The buffer has
+// at least 16 bytes of padding, so the second word never leaves it.
+struct Bits {
+    const uint64_t *w;
+    uint64_t pos, end, idx, w0, w1;
+
+    __device__ __forceinline__ uint64_t ld(uint64_t i) const { return bswap64(__ldg(w + i)); }
+    __device__ __forceinline__ void init(const uint8_t *base, uint64_t byte_off, uint64_t len) {
+        w = reinterpret_cast<const uint64_t *>(base);
+        pos = byte_off * 8;
+        end = pos + len * 8;
+        idx = pos >> 6;
+        w0 = ld(idx);
+        w1 = ld(idx + 1);
+    }
+    __device__ __forceinline__ uint64_t remaining() const { return end - pos; }
+    __device__ __forceinline__ uint64_t peek() {
+        uint64_t i = pos >> 6;
+        if (i != idx) {
+            if (i == idx + 1) {
+                w0 = w1;
+                w1 = ld(i + 1);
+            } else {
+                w0 = ld(i);
+                w1 = ld(i + 1);
+            }
+            idx = i;
+        }
+        uint32_t sh = (uint32_t)(pos & 63);
+        uint64_t v = sh ? (w0 << sh) | (w1 >> (64 - sh)) : w0;
+        uint64_t rem = end - pos;
+        if (rem < 64) v &= rem ? (~0ull << (64 - rem)) : 0ull;
+        return v;
+    }
+    // `n` (1..57) bits as a number (src/bits.rs:61-72).
+    __device__ __forceinline__ int read(uint32_t n, uint64_t &v) {
+        if ((uint64_t)n > remaining()) return DE_PAST_END;
+        v = peek() >> (64 - n);
+        pos += n;
+        return DE_OK;
+    }
+    // RDD 36 endOfData(): 31 or fewer bits remain, all zero (src/bits.rs:98-101).
+    __device__ __forceinline__ bool end_of_data() {
+        return remaining() <= 31 && peek() == 0;
+    }
+};
+
+// One symbol of codebook `cb` (src/vlc.rs:207-230), with a prefix-table
+// shortcut for codewords of 9 bits or fewer that lie wholly inside the data
+// (those decode the same either way; anything else takes the general path,
+// which also names the failure exactly as the crate does).
+__device__ __forceinline__ int read_sym(Bits &b, const uint16_t *tab, Codebook cb, uint32_t &sym) {
+    uint64_t w = b.peek();
+    uint64_t rem = b.remaining();
+    if (tab) {
+        uint32_t e = tab[w >> (64 - kDecodeBits)];
+        uint32_t l = e & 31;
+        if (e && l <= rem) {
+            sym = e >> 5;
+            b.pos += l;
+            return DE_OK;
+        }
+    }
+    uint32_t lz = clz64(w);
+    if (lz > kMaxPrefix) return DE_PREFIX;
+    if ((uint64_t)lz >= rem) return DE_PAST_END;
+    b.pos += lz;
+    rem -= lz;
+    w = b.peek();
+    if (!cb.eg && lz <= cb.q) {
+        uint32_t need = 1u + cb.r;
+        if (need > rem) return DE_PAST_END;
+        uint64_t v = (w >> (64 - need)) & ((1ull << cb.r) - 1);
+        b.pos += need;
+        sym = (uint32_t)(((uint64_t)lz << cb.r) | v);
+        return DE_OK;
+    }
+    uint32_t qe = cb.eg ? lz : lz - (cb.q + 1u);
+    uint32_t ke = cb.eg ? cb.r : cb.e;
+    uint64_t off = cb.eg ? 0ull : ((uint64_t)(cb.q + 1u) << cb.r);
+    uint32_t need = qe + ke + 1u;
+    if (need > rem) return DE_PAST_END;
+    uint64_t v = w >> (64 - need);
+    b.pos += need;
+    uint64_t n = v - (1ull << ke) + off;
+    if (n > kMaxSymbol) return DE_RANGE;
+    sym = (uint32_t)n;
+    return DE_OK;
+}
+
+// scanned_coefficients() of one component (src/decode.rs:484-540) into the
+// scratch in scanned order (index n of n_blocks * 64).
+__device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const uint16_t *run_tab,
+                                const uint16_t *level_tab) {
+    uint32_t sym;
+    int err = read_sym(b, nullptr, kFirstDcBook, sym);
+    if (err) return err;
+    int32_t prev_dc = symbol_to_signed(sym);
+    out[0] = prev_dc;
+    int32_t prev_diff = 3;
+    for (uint32_t i = 1; i < n_blocks; i++) {
+        if ((err = read_sym(b, nullptr, dc_book(prev_diff), sym))) return err;
+        int32_t n = symbol_to_signed(sym);
+        int32_t diff = prev_diff < 0 ? -n : n;
+        int64_t s = (int64_t)prev_dc + diff;
+        if (s > INT32_MAX || s < INT32_MIN) return DE_DC_OVERFLOW;
+        prev_dc = (int32_t)s;
+        out[i] = prev_dc;
+        prev_diff = diff;
+    }
+    const uint32_t total = n_blocks * 64;
+    uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
+    for (;;) {
+        uint64_t rem = b.remaining();
+        uint64_t w = b.peek();
+        if (rem >= 64) {
+            // Run, level and sign from one window when both codewords are
+            // in the prefix tables (all 64 window bits are data here).
+            uint32_t e1 = run_tab[(prev_run < 15u ? prev_run : 15u) * kDecodeEntries + (w >> (64 - kDecodeBits))];
+            if (e1) {
+                uint32_t l1 = e1 & 31;
+                uint64_t w2 = w << l1;
+                uint32_t e2 =
+                    level_tab[(prev_level < 8u ? prev_level : 8u) * kDecodeEntries + (w2 >> (64 - kDecodeBits))];
+                if (e2) {
+                    uint32_t l2 = e2 & 31;
+                    uint32_t run = e1 >> 5, lvl = e2 >> 5;
+                    n += run;
+                    if (n >= total) return DE_RUN_PAST_END;
+                    int32_t level = (int32_t)lvl + 1;
+                    bool neg = (w2 << l2) >> 63;
+                    b.pos += l1 + l2 + 1;
+                    out[n] = neg ? -level : level;
+                    n += 1;
+                    prev_run = run;
+                    prev_level = lvl;
+                    continue;
+                }
+            }
+        } else if (rem <= 31 && w == 0) {
+            break;  // endOfData()
+        }
+        uint32_t run, lvl;
+        if ((err = read_sym(b, run_tab + (prev_run < 15u ? prev_run : 15u) * kDecodeEntries, run_book(prev_run),
+                            run)))
+            return err;
+        prev_run = run;
+        n += run;
+        if (n >= total || run >= total) return DE_RUN_PAST_END;
+        if ((err = read_sym(b, level_tab + (prev_level < 8u ? prev_level : 8u) * kDecodeEntries,
+                            level_book(prev_level), lvl)))
+            return err;
+        prev_level = lvl;
+        if (b.remaining() < 1) return DE_PAST_END;
+        bool neg = b.peek() >> 63;
+        b.pos += 1;
+        int32_t level = (int32_t)lvl + 1;
+        out[n] = neg ? -level : level;
+        n += 1;
+    }
+    return DE_OK;
+}
+
+__device__ __forceinline__ uint16_t rescale(uint32_t a, uint64_t m, bool identity) {
+    return identity ? (uint16_t)a : (uint16_t)(((uint64_t)a * m + (1ull << 39)) >> 40);
+}
+
+// scanned_alpha() (src/decode.rs:570-595) and its placement (:365-389).
+__device__ int decode_alpha(Bits &b, const FrameDesc &fd, const PicDesc &pd, const SliceDesc &sd, uint16_t *alpha) {
+    const uint32_t bits = fd.alpha_bits;
+    const uint32_t cols = 16u * sd.mbs;
+    const uint32_t count = cols * 16u;
+    const uint32_t rows = (uint32_t)sd.mb_y + 1u < pd.height_in_mb ? 16u : pd.height - 16u * (pd.height_in_mb - 1u);
+    const uint32_t needed = cols * rows;
+    const uint32_t width = fd.width;
+    const uint32_t x0 = 16u * sd.mb_x;
+    const uint32_t ncols = min(cols, width - x0);
+    const int32_t mask = (int32_t)((1u << bits) - 1u);
+    const uint32_t mag_bits = bits == 8 ? 3u : 6u;
+    uint16_t *plane = alpha + fd.alpha_off;
+    int32_t prev = -1;
+    uint32_t n = 0;
+    int err;
+    while (n < count) {
+        if (n >= needed && b.end_of_data()) break;
+        uint64_t v;
+        int32_t diff;
+        if ((err = b.read(1, v))) return err;
+        if (v == 1) {
+            if ((err = b.read(bits, v))) return err;
+            diff = (int32_t)v;
+        } else {
+            if ((err = b.read(mag_bits, v))) return err;
+            int32_t a = (int32_t)v + 1;
+            if ((err = b.read(1, v))) return err;
+            diff = v ? -a : a;
+        }
+        int32_t value = (int32_t)((uint32_t)prev + (uint32_t)diff) & mask;
+        prev = value;
+        uint32_t run;
+        if ((err = b.read(1, v))) return err;
+        if (v == 1) {
+            run = 1;
+        } else {
+            if ((err = b.read(4, v))) return err;
+            if (v != 0) {
+                run = (uint32_t)v + 1;
+            } else {
+                if ((err = b.read(11, v))) return err;
+                run = (uint32_t)v + 1;
+            }
+        }
+        if (n + run > count) return DE_ALPHA_RUN;
+        uint16_t out = rescale((uint32_t)value, fd.rescale_m, fd.rescale_identity != 0);
+        uint32_t stop = min(n + run, needed);
+        for (uint32_t i = n; i < stop;) {
+            uint32_t r = i / cols, c = i - r * cols;
+            uint32_t seg_end = min(stop - i, cols - c);  // samples left in this row of the run
+            uint16_t *row = plane + (uint64_t)(pd.first_row + pd.row_step * (16u * sd.mb_y + r)) * width + x0;
+            for (uint32_t k = c; k < c + seg_end && k < ncols; k++) row[k] = out;
+            i += seg_end;
+        }
+        n += run;
+    }
+    return DE_OK;
+}
+
+// One work item: component `comp` (0 Y', 1 Cb, 2 Cr, 3 alpha) of slice `s`.
+__device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, const uint16_t *run_tab,
+                            const uint16_t *level_tab) {
+    int2 *slot = d.slot_status + 4ull * s + comp;
+    const SliceDesc sd = d.slices[s];
+    const PicDesc &pd = d.pics[sd.pic];
+    if (d.pic_status[sd.pic].locate_slice >= 0) return;  // never read: the picture failed before decoding
+    const FrameDesc &fd = d.frames[pd.frame];
+    const bool has_alpha = fd.alpha_bits != 0;
+    if (comp == 3 && !has_alpha) {
+        *slot = make_int2(DE_OK, 0);
+        return;
+    }
+    // The slice header (src/decode.rs:301-338); the Y' item reports it.
+    const uint8_t *sb = d.bits + sd.off;
+    const uint32_t size = sd.size;
+    const uint32_t min_header = has_alpha ? 8u : 6u;
+    int2 hdr_err = make_int2(DE_OK, 0);
+    uint32_t hs = 0, ys = 0, cbs = 0, crs = 0;
+    if (size < min_header) {
+        hdr_err = make_int2(DE_SLICE_SHORT, 0);
+    } else {
+        hs = sb[0] >> 3;
+        uint32_t qi = sb[1];
+        if (hs < min_header || hs > size) {
+            hdr_err = make_int2(DE_SLICE_HDR_SIZE, (int)hs);
+        } else if (qi < 1 || qi > 224) {
+            hdr_err = make_int2(DE_QINDEX, (int)qi);
+        } else {
+            ys = be16(sb + 2);
+            cbs = be16(sb + 4);
+            uint32_t body = size - hs;
+            if (has_alpha) {
+                crs = be16(sb + 6);
+            } else if (ys + cbs > body) {
+                hdr_err = make_int2(DE_COMP_SIZES, 0);
+            } else {
+                crs = body - ys - cbs;
+            }
+            if (hdr_err.x == DE_OK && ys + cbs + crs > body) hdr_err = make_int2(DE_COMP_SIZES, 0);
+        }
+    }
+    if (hdr_err.x != DE_OK) {
+        *slot = comp == 0 ? hdr_err : make_int2(DE_OK, 0);
+        return;
+    }
+    uint32_t start = hs, len;
+    if (comp == 0) {
+        len = ys;
+    } else if (comp == 1) {
+        start += ys;
+        len = cbs;
+    } else if (comp == 2) {
+        start += ys + cbs;
+        len = crs;
+    } else {
+        start += ys + cbs + crs;
+        len = size - start;
+    }
+    Bits b;
+    b.init(d.bits, sd.off + start, len);
+    int err;
+    if (comp == 3) {
+        err = decode_alpha(b, fd, pd, sd, d.alpha);
+    } else {
+        const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+        const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
+        const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
+        err = decode_component(b, n_blocks, d.coef + base, run_tab, level_tab);
+    }
+    *slot = make_int2(err, 0);
+}
+
+// ------------------------------------------------------------------ kernels
+
+constexpr int kLocateThreads = 1024;
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kLocateThreads) k_locate(DecodeLaunch d) {
+    __shared__ uint32_t warp_sums[kLocateThreads / 32];
+    __shared__ uint64_t carry;
+    __shared__ int first_bad;
+    const PicDesc p = d.pics[blockIdx.x];
+    const FrameDesc &fd = d.frames[p.frame];
+    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+    const uint32_t coef_per_mb = 64u * (4u + 2u * cpm);
+    const uint32_t S = 1u << p.log2_slice_mbs;
+    const uint32_t full = p.width_in_mb >> p.log2_slice_mbs;
+    const uint32_t rem_mbs = p.width_in_mb & (S - 1u);
+    const uint8_t *table = d.bits + p.off + p.header_size;
+    const uint64_t data_start = p.off + p.header_size + 2ull * p.n_slices;
+    const uint64_t limit = p.off + p.picture_size;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        first_bad = INT32_MAX;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t chunk = 0; chunk < p.n_slices; chunk += kLocateThreads) {
+        const uint32_t k = chunk + threadIdx.x;
+        const uint32_t size = k < p.n_slices ? be16(table + 2ull * k) : 0u;
+        uint32_t incl = warp_incl_scan(size);
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t ws = warp_sums[lane];
+            warp_sums[lane] = warp_incl_scan(ws);
+        }
+        __syncthreads();
+        const uint64_t excl = carry + (warp ? warp_sums[warp - 1] : 0u) + incl - size;
+        if (k < p.n_slices) {
+            const uint64_t off = data_start + excl;
+            if (off + size > limit) atomicMin(&first_bad, (int)k);
+            const uint32_t row = k / p.slices_per_row, j = k - row * p.slices_per_row;
+            uint32_t mb_x, mbs;
+            if (j < full) {
+                mb_x = j * S;
+                mbs = S;
+            } else {
+                // The slices after the full ones halve down the binary digits
+                // of what is left (src/header.rs:308-320).
+                uint32_t idx = j - full;
+                mb_x = full * S;
+                mbs = 1;
+                for (int bit = (int)p.log2_slice_mbs - 1; bit >= 0; bit--) {
+                    if (!(rem_mbs & (1u << bit))) continue;
+                    if (idx == 0) {
+                        mbs = 1u << bit;
+                        break;
+                    }
+                    mb_x += 1u << bit;
+                    idx--;
+                }
+            }
+            SliceDesc sd;
+            sd.off = off;
+            sd.size = size;
+            sd.pic = blockIdx.x;
+            sd.mb_x = (uint16_t)mb_x;
+            sd.mb_y = (uint16_t)row;
+            sd.mbs = mbs;
+            sd.coef = p.coef_base + ((uint64_t)row * p.width_in_mb + mb_x) * coef_per_mb;
+            d.slices[p.slice_base + k] = sd;
+        }
+        __syncthreads();
+        if (threadIdx.x == kLocateThreads - 1) carry += (warp ? warp_sums[warp - 1] : 0u) + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        PicStatus st;
+        st.locate_slice = first_bad == INT32_MAX ? -1 : first_bad;
+        st.slot = -1;
+        st.code = 0;
+        st.aux = 0;
+        d.pic_status[blockIdx.x] = st;
+    }
+}
+
+constexpr int kEntropyThreads = 256;
+
+__global__ void __launch_bounds__(kEntropyThreads) k_entropy(DecodeLaunch d) {
+    __shared__ uint16_t run_tab[kRunTableWords];
+    __shared__ uint16_t level_tab[kLevelTableWords];
+    for (uint32_t i = threadIdx.x; i < kRunTableWords / 2; i += blockDim.x)
+        reinterpret_cast<uint32_t *>(run_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.run_decode)[i];
+    for (uint32_t i = threadIdx.x; i < kLevelTableWords / 2; i += blockDim.x)
+        reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_decode)[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t items = 4u * d.n_slices;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(d.work_counter, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= items) break;
+        const uint32_t item = base + lane;
+        if (item < items) {
+            const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
+            decode_item(d, comp, s, run_tab, level_tab);
+        }
+        __syncwarp();
+    }
+}
+
+constexpr int kIdctThreads = 256;
+constexpr int kMaxSliceCoefs = 64 * 12 * 8;  // 8 macroblocks of 4:4:4
+
+// Placement of block b of macroblock m (src/decode.rs:395-413).
+__device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_t mb_x, uint32_t mb_y, uint32_t m,
+                                         uint32_t b, uint32_t &bx, uint32_t &by) {
+    const uint32_t x = mb_x + m, y0 = 16u * mb_y;
+    if (comp == 0) {
+        bx = 16u * x + 8u * (b & 1u);
+        by = y0 + 8u * (b >> 1);
+    } else if (chroma == 2) {
+        bx = 8u * x;
+        by = y0 + 8u * b;
+    } else {
+        bx = 16u * x + 8u * (b >> 1);
+        by = y0 + 8u * (b & 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kIdctThreads) k_idct(DecodeLaunch d) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int32_t *cs = reinterpret_cast<int32_t *>(smem);                   // scanned coefficients
+    float *tmp = reinterpret_cast<float *>(smem + 4 * kMaxSliceCoefs);  // row pass, [v][x][blk] per component
+    uint8_t *nz = smem + 8 * kMaxSliceCoefs;                           // non-zero rows, [blk][v]
+    __shared__ float scale[2][64];
+    __shared__ float basis[64];
+    __shared__ uint8_t scan[64];
+
+    const SliceDesc sd = d.slices[blockIdx.x];
+    const PicDesc &pd = d.pics[sd.pic];
+    if (d.pic_status[sd.pic].locate_slice >= 0) return;
+    const FrameDesc &fd = d.frames[pd.frame];
+    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+    const uint32_t mbs = sd.mbs;
+    const uint32_t total = 64u * (4u + 2u * cpm) * mbs;
+    const uint32_t tid = threadIdx.x;
+
+    // Load the slice's scanned coefficients and leave the scratch zeroed.
+    int4 *g4 = reinterpret_cast<int4 *>(d.coef + sd.coef);
+    int4 *s4 = reinterpret_cast<int4 *>(cs);
+    for (uint32_t i = tid; i < total / 4; i += kIdctThreads) {
+        s4[i] = g4[i];
+        g4[i] = make_int4(0, 0, 0, 0);
+    }
+    uint32_t qi = sd.size >= 2 ? d.bits[sd.off + 1] : 1u;
+    qi = qi < 1u ? 1u : (qi > 224u ? 224u : qi);
+    const uint32_t q = qscale(qi);
+    if (tid < 128) {
+        const uint32_t which = tid >> 6, k = tid & 63;
+        // F = QF * (W * qScale / 8), one factor per raster position (src/decode.rs:356).
+        scale[which][k] = (float)((uint32_t)d.weights[fd.weights * 128u + which * 64u + k] * q) / 8.0f;
+    } else if (tid < 192) {
+        basis[tid - 128] = d.tables.basis[tid - 128];
+    } else {
+        scan[tid - 192] = c_scan[pd.interlaced_scan][tid - 192];
+    }
+    __syncthreads();
+
+    // Row pass: tmp[v][x] = sum_u F[v][u] T[x][u], u in order, from 0
+    // (src/dct.rs:38-53); all-zero rows are skipped, as the crate does.
+    uint32_t comp_start[3], comp_blocks[3];
+    comp_blocks[0] = 4u * mbs;
+    comp_blocks[1] = comp_blocks[2] = cpm * mbs;
+    comp_start[0] = 0;
+    comp_start[1] = 64u * comp_blocks[0];
+    comp_start[2] = comp_start[1] + 64u * comp_blocks[1];
+    const uint32_t all_blocks = comp_blocks[0] + 2u * comp_blocks[1];
+    for (uint32_t t = tid; t < all_blocks * 8u; t += kIdctThreads) {
+        const uint32_t c = t < comp_blocks[0] * 8u ? 0u : (t < (comp_blocks[0] + comp_blocks[1]) * 8u ? 1u : 2u);
+        const uint32_t tc = t - (c == 0 ? 0u : (c == 1 ? comp_blocks[0] * 8u : (comp_blocks[0] + comp_blocks[1]) * 8u));
+        const uint32_t nb = comp_blocks[c];
+        const uint32_t blk = tc % nb, v = tc / nb;
+        const int32_t *src = cs + comp_start[c];
+        const float *sc = scale[c > 0];
+        float row[8];
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const uint32_t k = 8u * v + u;
+            row[u] = __fmul_rn(__int2float_rn(src[nb * scan[k] + blk]), sc[k]);
+            any |= row[u] != 0.0f;
+        }
+        const uint32_t gblk = comp_start[c] / 64u + blk;
+        nz[gblk * 8u + v] = any;
+        if (any) {
+            float *dst = tmp + comp_start[c];
+#pragma unroll
+            for (int x = 0; x < 8; x++) {
+                float s = 0.0f;
+#pragma unroll
+                for (int u = 0; u < 8; u++) s = __fadd_rn(s, __fmul_rn(row[u], basis[8 * x + u]));
+                dst[(v * 8u + x) * nb + blk] = s;
+            }
+        }
+    }
+    __syncthreads();
+
+    // Column pass, conversion and store: out[y][x] = sum_v T[y][v] tmp[v][x]
+    // in order (src/dct.rs:54-64), then floor(v scale + bias) clamped
+    // (src/dsp/scalar.rs:8-12). A thread makes one 8-sample row of a block;
+    // neighbouring threads make neighbouring rows segments of the picture.
+    const float oscale = fd.out_scale, obias = fd.out_bias, omax = fd.out_max;
+    for (uint32_t c = 0; c < 3; c++) {
+        const uint32_t segs = (c == 0 || cpm == 4) ? 2u * mbs : mbs;
+        const uint32_t per_mb = c == 0 ? 4u : cpm;
+        const uint32_t nb = comp_blocks[c];
+        const uint32_t pw = fd.plane_w[c];
+        uint16_t *plane = d.planes + fd.plane_off[c];
+        for (uint32_t t = tid; t < 16u * segs; t += kIdctThreads) {
+            const uint32_t r = t / segs, sx = t - r * segs;
+            uint32_t m, bb;
+            if (c == 0) {
+                m = sx >> 1;
+                bb = ((r >> 3) << 1) | (sx & 1u);
+            } else if (cpm == 2) {
+                m = sx;
+                bb = r >> 3;
+            } else {
+                m = sx >> 1;
+                bb = ((sx & 1u) << 1) | (r >> 3);
+            }
+            const uint32_t blk = m * per_mb + bb, y = r & 7u;
+            uint32_t bx, by;
+            block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, bb, bx, by);
+            if (bx >= pw || by + y >= pd.height) continue;
+            const uint32_t gblk = comp_start[c] / 64u + blk;
+            const float *src = tmp + comp_start[c];
+            float acc[8];
+#pragma unroll
+            for (int x = 0; x < 8; x++) acc[x] = 0.0f;
+#pragma unroll
+            for (int v = 0; v < 8; v++) {
+                if (!nz[gblk * 8u + v]) continue;
+                const float w = basis[8u * y + v];
+#pragma unroll
+                for (int x = 0; x < 8; x++) acc[x] = __fadd_rn(acc[x], __fmul_rn(w, src[(v * 8u + x) * nb + blk]));
+            }
+            uint16_t px[8];
+#pragma unroll
+            for (int x = 0; x < 8; x++) {
+                float s = floorf(__fadd_rn(__fmul_rn(acc[x], oscale), obias));
+                s = s < 0.0f ? 0.0f : (s > omax ? omax : s);
+                px[x] = (uint16_t)s;
+            }
+            const uint32_t cols = min(8u, pw - bx);
+            uint16_t *dst = plane + (uint64_t)(pd.first_row + pd.row_step * (by + y)) * pw + bx;
+            if (cols == 8u && ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0)) {
+                uint4 v;
+                v.x = px[0] | ((uint32_t)px[1] << 16);
+                v.y = px[2] | ((uint32_t)px[3] << 16);
+                v.z = px[4] | ((uint32_t)px[5] << 16);
+                v.w = px[6] | ((uint32_t)px[7] << 16);
+                *reinterpret_cast<uint4 *>(dst) = v;
+            } else {
+                for (uint32_t x = 0; x < cols; x++) dst[x] = px[x];
+            }
+        }
+    }
+}
+
+constexpr int kStatusThreads = 256;
+
+__global__ void __launch_bounds__(kStatusThreads) k_status(DecodeLaunch d) {
+    __shared__ int best;
+    const PicDesc p = d.pics[blockIdx.x];
+    if (threadIdx.x == 0) best = INT32_MAX;
+    __syncthreads();
+    if (d.pic_status[blockIdx.x].locate_slice < 0) {
+        const uint64_t first = 4ull * p.slice_base, n = 4ull * p.n_slices;
+        for (uint64_t i = threadIdx.x; i < n; i += kStatusThreads) {
+            if (d.slot_status[first + i].x != DE_OK) {
+                atomicMin(&best, (int)i);
+                break;  // later slots of this thread are further on
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && best != INT32_MAX) {
+        const int2 st = d.slot_status[4ull * p.slice_base + best];
+        d.pic_status[blockIdx.x].slot = best;
+        d.pic_status[blockIdx.x].code = st.x;
+        d.pic_status[blockIdx.x].aux = st.y;
+    }
+}
+
+}  // namespace
+
+cudaError_t upload_scans() {
+    uint8_t s[2][64];
+    for (int i = 0; i < 64; i++) {
+        s[0][i] = kProgressiveScan[i];
+        s[1][i] = kInterlacedScan[i];
+    }
+    return cudaMemcpyToSymbol(c_scan, s, sizeof s);
+}
+
+cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s) {
+    if (d.n_pics == 0) return cudaSuccess;
+    k_locate<<<d.n_pics, kLocateThreads, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_entropy(const DecodeLaunch &d, int grid, cudaStream_t s) {
+    if (d.n_slices == 0) return cudaSuccess;
+    k_entropy<<<grid, kEntropyThreads, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+size_t idct_smem_bytes() { return 8 * kMaxSliceCoefs + 8 * (kMaxSliceCoefs / 64); }
+
+cudaError_t launch_idct(const DecodeLaunch &d, cudaStream_t s) {
+    if (d.n_slices == 0) return cudaSuccess;
+    k_idct<<<d.n_slices, kIdctThreads, idct_smem_bytes(), s>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s) {
+    if (d.n_pics == 0) return cudaSuccess;
+    k_status<<<d.n_pics, kStatusThreads, 0, s>>>(d);
+    return cudaGetLastError();
+}
+
+cudaError_t configure_decode_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(k_idct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)idct_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return upload_scans();
+}
+
+int entropy_grid(int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_entropy, kEntropyThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+}  // namespace prores

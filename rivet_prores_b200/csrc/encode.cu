@@ -1,0 +1,900 @@
+// encode.cu -- the encoder (the crate's src/encode.rs) as sm_100a kernels.
+//
+//   k_fdct        one CTA per slice: edge-replicated 8x8 gathers, p = s 512/2^b
+//                 - 256 and the FDCT in the crate's exact single-precision
+//                 order (src/encode.rs:488-555, src/dct.rs:70-93), written in
+//                 the slice's scanned order once per frame.
+//   k_alpha_size  one warp per slice: the lossless alpha codes' size
+//                 (src/encode.rs:838-868, :457-470); it does not depend on
+//                 the quantiser.
+//   k_rc_init / k_cost / k_rc_step
+//                 the rate control's probe sequence replayed exactly: 224,
+//                 then mid = lo + (hi - lo) / 2 while lo < hi
+//                 (src/encode.rs:685-713). k_cost sizes every slice of every
+//                 picture still searching at that picture's probe, one warp
+//                 per slice component (quantise + exact bit count,
+//                 src/dsp/scalar.rs:19-39, src/encode.rs:398-409); k_rc_step
+//                 sums a picture's slices and moves its interval.
+//   k_cost_window the next kWindow finer quantisers below the uniform one.
+//   k_shareout    one warp per picture: the sequential share-out of the slack
+//                 (src/encode.rs:769-793), costing any deeper quantiser it
+//                 needs itself.
+//   k_layout / k_frame
+//                 slice offsets (an exclusive scan per picture), picture and
+//                 frame sizes, the frame and picture headers.
+//   k_pack        one CTA per slice: the slice header, the table entry, and
+//                 each component's codes bit-packed straight into the frame
+//                 (src/encode.rs:413-437, :797-829), plus the alpha codes.
+//
+// Output bits are OR-ed into a zeroed buffer as big-endian 32-bit words, so
+// writers that share a word never need to be ordered.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "codec_tables.h"
+#include "encode_types.h"
+
+namespace prores {
+
+__constant__ uint8_t c_enc_scan[2][64];
+
+namespace {
+
+constexpr float kAcRounding = 0.42f;  // src/encode.rs:204
+
+__device__ __forceinline__ uint32_t bswap32(uint32_t v) { return __byte_perm(v, 0, 0x0123); }
+
+// ORs `value` into the bit field [bitpos, bitpos + len) (MSB first; the
+// value's leading zeros are the field's) of a big-endian bit buffer.
+__device__ __forceinline__ void put_field(uint32_t *out, uint64_t bitpos, uint64_t value, uint32_t len) {
+    const uint32_t nb = bit_len64(value);
+    if (nb == 0) return;
+    const uint64_t start = bitpos + len - nb;
+    uint32_t *w = out + (start >> 5);
+    const uint32_t o = (uint32_t)(start & 31);
+    const uint32_t first = 32 - o;
+    if (nb <= first) {
+        atomicOr(w, bswap32((uint32_t)(value << (first - nb))));
+        return;
+    }
+    const uint32_t rest = nb - first;
+    atomicOr(w, bswap32((uint32_t)(value >> rest)));
+    if (rest <= 32) {
+        atomicOr(w + 1, bswap32((uint32_t)(value << (32 - rest))));
+    } else {
+        atomicOr(w + 1, bswap32((uint32_t)(value >> (rest - 32))));
+        atomicOr(w + 2, bswap32((uint32_t)(value << (64 - rest))));
+    }
+}
+
+__device__ __forceinline__ int32_t quantise1(float f, float inv, float r) {
+    // x = F inv; QF = sign(x) floor(|x| + r) (src/dsp/scalar.rs:19-39).
+    const float x = __fmul_rn(f, inv);
+    const float m = floorf(__fadd_rn(fabsf(x), r));
+    const int32_t q = __float2int_rz(m);
+    return x < 0.0f ? -q : q;
+}
+
+// ---------------------------------------------------------------- fdct
+
+constexpr int kFdctThreads = 256;
+constexpr int kMaxSliceCoefs = 64 * 12 * 8;
+
+__device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_t mb_x, uint32_t mb_y, uint32_t m,
+                                         uint32_t b, uint32_t &bx, uint32_t &by) {
+    const uint32_t x = mb_x + m, y0 = 16u * mb_y;
+    if (comp == 0) {
+        bx = 16u * x + 8u * (b & 1u);
+        by = y0 + 8u * (b >> 1);
+    } else if (chroma == 2) {
+        bx = 8u * x;
+        by = y0 + 8u * b;
+    } else {
+        bx = 16u * x + 8u * (b >> 1);
+        by = y0 + 8u * (b & 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
+    __shared__ float tmp[kMaxSliceCoefs];  // [comp][y][u][blk]
+    __shared__ float basis[64];
+    __shared__ uint8_t scan[64];
+    const EncSliceDesc sd = e.slices[blockIdx.x];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const uint32_t tid = threadIdx.x;
+    if (tid < 64) basis[tid] = e.basis[tid];
+    else if (tid < 128) scan[tid - 64] = c_enc_scan[pd.interlaced_scan][tid - 64];
+    __syncthreads();
+    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+    const uint32_t mbs = sd.mbs;
+    uint32_t nbk[3], start[3];
+    nbk[0] = 4u * mbs;
+    nbk[1] = nbk[2] = cpm * mbs;
+    start[0] = 0;
+    start[1] = 64u * nbk[0];
+    start[2] = start[1] + 64u * nbk[1];
+    const float scale = fd.in_scale;
+
+    // Pass 1: tmp[y][u] = sum_x p[y][x] T[x][u], x in order from 0.
+    for (uint32_t c = 0; c < 3; c++) {
+        const uint32_t segs = (c == 0 || cpm == 4) ? 2u * mbs : mbs;
+        const uint32_t per_mb = c == 0 ? 4u : cpm;
+        const uint32_t w = fd.plane_w[c];
+        const uint16_t *plane = e.in + fd.in_off[c];
+        for (uint32_t t = tid; t < 16u * segs; t += kFdctThreads) {
+            const uint32_t r = t / segs, sx = t - r * segs;
+            uint32_t m, bb;
+            if (c == 0) {
+                m = sx >> 1;
+                bb = ((r >> 3) << 1) | (sx & 1u);
+            } else if (cpm == 2) {
+                m = sx;
+                bb = r >> 3;
+            } else {
+                m = sx >> 1;
+                bb = ((sx & 1u) << 1) | (r >> 3);
+            }
+            const uint32_t blk = m * per_mb + bb, y = r & 7u;
+            uint32_t bx, by;
+            block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, bb, bx, by);
+            // Edge replication: the last picture row and column repeat.
+            const uint32_t py = min(by + y, pd.height - 1u);
+            const uint16_t *line = plane + (uint64_t)(pd.first_row + pd.row_step * py) * w;
+            float p[8];
+            if (bx + 8u <= w && ((reinterpret_cast<uintptr_t>(line + bx) & 15u) == 0)) {
+                const uint4 v = *reinterpret_cast<const uint4 *>(line + bx);
+                const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    p[2 * i] = __fsub_rn(__fmul_rn((float)(words[i] & 0xFFFFu), scale), 256.0f);
+                    p[2 * i + 1] = __fsub_rn(__fmul_rn((float)(words[i] >> 16), scale), 256.0f);
+                }
+            } else {
+#pragma unroll
+                for (int x = 0; x < 8; x++) {
+                    const uint32_t col = min(bx + (uint32_t)x, w - 1u);
+                    p[x] = __fsub_rn(__fmul_rn((float)line[col], scale), 256.0f);
+                }
+            }
+            const uint32_t nb = nbk[c];
+            float *dst = tmp + start[c];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                float s = 0.0f;
+#pragma unroll
+                for (int x = 0; x < 8; x++) s = __fadd_rn(s, __fmul_rn(p[x], basis[8 * x + u]));
+                dst[(y * 8u + u) * nb + blk] = s;
+            }
+        }
+    }
+    __syncthreads();
+
+    // Pass 2: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0, written
+    // to the scanned position n * scan[8v + u] + blk of the component.
+    float *gout = e.coef + sd.coef;
+    for (uint32_t c = 0; c < 3; c++) {
+        const uint32_t nb = nbk[c];
+        const float *src = tmp + start[c];
+        for (uint32_t t = tid; t < 8u * nb; t += kFdctThreads) {
+            const uint32_t blk = t % nb, u = t / nb;
+            float col[8];
+#pragma unroll
+            for (int y = 0; y < 8; y++) col[y] = src[(y * 8u + u) * nb + blk];
+#pragma unroll
+            for (int v = 0; v < 8; v++) {
+                float s = 0.0f;
+#pragma unroll
+                for (int y = 0; y < 8; y++) s = __fadd_rn(s, __fmul_rn(basis[8 * y + v], col[y]));
+                gout[start[c] + nb * scan[8 * v + u] + blk] = s;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- alpha
+
+constexpr int kAlphaWarps = 4;
+constexpr int kMaxAlphaValues = 16 * 16 * 8;
+
+struct AlphaScratch {
+    uint16_t start[kMaxAlphaValues + 1];
+    uint16_t value[kMaxAlphaValues];
+};
+
+__device__ __forceinline__ uint32_t alpha_diff_len(int32_t diff, uint32_t bits) {
+    const uint32_t a = diff < 0 ? 0u - (uint32_t)diff : (uint32_t)diff;
+    const uint32_t mag = bits == 8 ? 3u : 6u, max = bits == 8 ? 8u : 64u;
+    return (a >= 1u && a <= max) ? 2u + mag : 1u + bits;
+}
+__device__ __forceinline__ uint32_t alpha_run_len(uint32_t run) { return run == 1u ? 1u : (run <= 16u ? 5u : 16u); }
+
+// The slice's alpha values (16 rows of 16 mbs, edges repeated, converted to
+// the coded bits) into runs; returns the run count. A run cannot pass 2048
+// values: a slice has at most 2048.
+__device__ uint32_t alpha_runs(const EncodeLaunch &e, const EncSliceDesc &sd, const EncPicDesc &pd,
+                               const EncFrameDesc &fd, AlphaScratch &sc) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t cols = 16u * sd.mbs, count = 16u * cols;
+    const uint32_t width = fd.width, x0 = 16u * sd.mb_x;
+    const uint16_t max_in = (uint16_t)(0xFFFFu >> (16u - fd.bit_depth));
+    const uint16_t *plane = e.alpha_in + fd.alpha_in_off;
+    uint32_t n_runs = 0;
+    uint32_t prev = 0;
+    for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t i = base + lane;
+        uint32_t v = 0;
+        if (i < count) {
+            const uint32_t r = i / cols, n = i - r * cols;
+            const uint32_t row = pd.first_row + pd.row_step * min(16u * sd.mb_y + r, pd.height - 1u);
+            uint32_t a = plane[(uint64_t)row * width + min(x0 + n, width - 1u)];
+            a = a < max_in ? a : max_in;
+            v = fd.rescale_identity ? a : (uint32_t)(((uint64_t)a * fd.rescale_m + (1ull << 39)) >> 40);
+        }
+        const uint32_t before = __shfl_up_sync(0xffffffffu, v, 1);
+        const uint32_t left = lane == 0 ? prev : before;
+        const bool is_start = i < count && (i == 0 || v != left);
+        const uint32_t mask = __ballot_sync(0xffffffffu, is_start);
+        if (is_start) {
+            const uint32_t idx = n_runs + __popc(mask & ((1u << lane) - 1u));
+            sc.start[idx] = (uint16_t)i;
+            sc.value[idx] = (uint16_t)v;
+        }
+        n_runs += __popc(mask);
+        prev = __shfl_sync(0xffffffffu, v, 31);
+    }
+    if (lane == 0) sc.start[n_runs] = (uint16_t)count;
+    __syncwarp();
+    return n_runs;
+}
+
+__device__ __forceinline__ uint32_t alpha_run_bits(const AlphaScratch &sc, uint32_t j, uint32_t bits, uint32_t &dlen) {
+    const int32_t prev = j ? (int32_t)sc.value[j - 1] : -1;
+    dlen = alpha_diff_len((int32_t)sc.value[j] - prev, bits);
+    return dlen + alpha_run_len((uint32_t)sc.start[j + 1] - sc.start[j]);
+}
+
+__global__ void __launch_bounds__(32 * kAlphaWarps) k_alpha_size(EncodeLaunch e) {
+    __shared__ AlphaScratch scratch[kAlphaWarps];
+    const uint32_t s = blockIdx.x * kAlphaWarps + (threadIdx.x >> 5);
+    if (s >= e.n_slices) return;
+    const int lane = threadIdx.x & 31;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    if (fd.alpha_bits == 0) {
+        if (lane == 0) e.alpha_bytes[s] = 0;
+        return;
+    }
+    AlphaScratch &sc = scratch[threadIdx.x >> 5];
+    const uint32_t n_runs = alpha_runs(e, sd, pd, fd, sc);
+    uint32_t bits = 0;
+    for (uint32_t j = lane; j < n_runs; j += 32) {
+        uint32_t dlen;
+        bits += alpha_run_bits(sc, j, fd.alpha_bits, dlen);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
+    if (lane == 0) e.alpha_bytes[s] = (bits + 7u) / 8u;
+}
+
+__device__ void alpha_write(const EncodeLaunch &e, const EncSliceDesc &sd, const EncPicDesc &pd,
+                            const EncFrameDesc &fd, AlphaScratch &sc, uint64_t bitpos) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_runs = alpha_runs(e, sd, pd, fd, sc);
+    const uint32_t bits = fd.alpha_bits;
+    uint64_t carry = 0;
+    for (uint32_t base = 0; base < n_runs; base += 32) {
+        const uint32_t j = base + lane;
+        uint32_t dlen = 0, len = 0;
+        if (j < n_runs) len = alpha_run_bits(sc, j, bits, dlen);
+        uint32_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (j < n_runs) {
+            const uint64_t at = bitpos + carry + incl - len;
+            const int32_t prev = j ? (int32_t)sc.value[j - 1] : -1;
+            const int32_t diff = (int32_t)sc.value[j] - prev;
+            const uint32_t a = diff < 0 ? 0u - (uint32_t)diff : (uint32_t)diff;
+            const uint32_t mag = bits == 8 ? 3u : 6u, max = bits == 8 ? 8u : 64u;
+            // Tables 13/14: `0`, |d| - 1, sign; or `1` and d mod 2^bits.
+            if (a >= 1u && a <= max)
+                put_field(e.out, at, ((uint64_t)(a - 1u) << 1) | (uint64_t)(diff < 0), dlen);
+            else
+                put_field(e.out, at, (1ull << bits) | ((uint32_t)diff & ((1u << bits) - 1u)), dlen);
+            // Table 12: `1`; `0` and 4 bits of run - 1; or 5 zeros and 11 bits.
+            const uint32_t run = (uint32_t)sc.start[j + 1] - sc.start[j];
+            put_field(e.out, at + dlen, run == 1u ? 1u : run - 1u, len - dlen);
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+}
+
+// ---------------------------------------------------------------- costing
+
+// Bits of one quantised component (src/encode.rs:383-409), one warp: lane l
+// takes scanned positions 32 k + l; each non-zero's run and its contexts
+// (the previous non-zero's run and level symbol) come from the lanes below
+// it or from what the last step carried.
+__device__ uint32_t component_bits(const float *f, uint32_t n_blocks, const float *inv) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = 64u * n_blocks;
+    const uint32_t shift = 31u - __clz(n_blocks);
+    uint32_t bits = 0;
+    int32_t carry_pos = (int32_t)n_blocks - 1;
+    uint32_t carry_run = 4, carry_level = 1;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t p = base + lane;
+        const uint32_t sidx = p >> shift;
+        const int32_t q = quantise1(f[p], __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
+        if (base == 0) {
+            // The DCs (n_blocks <= 32, all in this step): EG5 of the first,
+            // then Table 9 by |previous difference|, sign flipped after a
+            // negative one.
+            const int32_t left = __shfl_up_sync(0xffffffffu, q, 1);
+            const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)left);
+            const int32_t prev_diff_raw = __shfl_up_sync(0xffffffffu, diff, 1);
+            if (p < n_blocks) {
+                if (p == 0) {
+                    bits += cb_len(kFirstDcBook, signed_to_symbol(q));
+                } else {
+                    const int32_t prev_diff = p == 1 ? 3 : prev_diff_raw;
+                    const int32_t n = prev_diff < 0 ? -diff : diff;
+                    bits += cb_len(dc_book(prev_diff), signed_to_symbol(n));
+                }
+            }
+        }
+        const bool nz = q != 0 && p >= n_blocks;
+        const uint32_t mask = __ballot_sync(0xffffffffu, nz);
+        if (mask == 0) continue;
+        const uint32_t below = mask & ((1u << lane) - 1u);
+        const int src = below ? 31 - __clz(below) : lane;
+        const int32_t prev_pos = below ? (int32_t)(base + src) : carry_pos;
+        const uint32_t run = nz ? (uint32_t)((int32_t)p - prev_pos - 1) : 0u;
+        const uint32_t level = nz ? (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u : 0u;
+        const uint32_t src_run = __shfl_sync(0xffffffffu, run, src);
+        const uint32_t src_level = __shfl_sync(0xffffffffu, level, src);
+        if (nz) {
+            const uint32_t ctx_run = below ? src_run : carry_run;
+            const uint32_t ctx_level = below ? src_level : carry_level;
+            bits += cb_len(run_book(ctx_run), run) + cb_len(level_book(ctx_level), level) + 1u;
+        }
+        const int top = 31 - __clz(mask);
+        carry_pos = (int32_t)(base + top);
+        carry_run = __shfl_sync(0xffffffffu, run, top);
+        carry_level = __shfl_sync(0xffffffffu, level, top);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
+    return bits;
+}
+
+__device__ __forceinline__ const float *quant_table(const EncodeLaunch &e, const EncPicDesc &pd, uint32_t qi,
+                                                    uint32_t comp) {
+    return e.quant + ((uint64_t)pd.quant * 225u + qi) * 128u + (comp > 0 ? 64u : 0u);
+}
+
+__device__ __forceinline__ void comp_layout(const EncFrameDesc &fd, uint32_t mbs, uint32_t comp, uint32_t &n_blocks,
+                                            uint32_t &offset) {
+    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+    n_blocks = (comp == 0 ? 4u : cpm) * mbs;
+    offset = comp == 0 ? 0u : 64u * mbs * (4u + (comp - 1u) * cpm);
+}
+
+// Bytes of one slice component at quantiser qi.
+__device__ __forceinline__ uint32_t component_bytes(const EncodeLaunch &e, const EncSliceDesc &sd, const EncPicDesc &pd,
+                                                    const EncFrameDesc &fd, uint32_t comp, uint32_t qi) {
+    uint32_t nb, off;
+    comp_layout(fd, sd.mbs, comp, nb, off);
+    const uint32_t bits = component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp));
+    return (bits + 7u) / 8u;
+}
+
+constexpr int kCostWarps = 8;
+
+__global__ void __launch_bounds__(32 * kCostWarps) k_cost(EncodeLaunch e, int step) {
+    const uint32_t item = blockIdx.x * kCostWarps + (threadIdx.x >> 5);
+    if (item >= 3u * e.n_slices) return;
+    const uint32_t s = item / 3u, comp = item - 3u * s;
+    const EncSliceDesc sd = e.slices[s];
+    const int32_t qi = e.state[sd.pic].probe_qi;
+    if (qi == 0) return;
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const uint32_t bytes = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi);
+    if ((threadIdx.x & 31) == 0) e.probe_comp[((uint64_t)step * e.n_slices + s) * 3u + comp] = bytes;
+}
+
+__global__ void __launch_bounds__(32 * kCostWarps) k_cost_window(EncodeLaunch e) {
+    const uint32_t item = blockIdx.x * kCostWarps + (threadIdx.x >> 5);
+    if (item >= 3u * kWindow * e.n_slices) return;
+    const uint32_t j = item / (3u * e.n_slices);
+    const uint32_t r = item - j * 3u * e.n_slices;
+    const uint32_t s = r / 3u, comp = r - 3u * s;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicState st = e.state[sd.pic];
+    if (!(st.fits_at_all && st.uniform > 1)) return;
+    const int32_t qi = st.uniform - 1 - (int32_t)j;
+    if (qi < 1) return;
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const uint32_t bytes = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi);
+    if ((threadIdx.x & 31) == 0) e.win_comp[((uint64_t)j * e.n_slices + s) * 3u + comp] = bytes;
+}
+
+// A slice's size from its component bytes, and whether every 16-bit size
+// field holds it (src/encode.rs:671-681).
+__device__ __forceinline__ uint64_t slice_total(uint32_t hdr, const uint32_t c[3], uint32_t alpha, bool &fits) {
+    const uint64_t t = (uint64_t)hdr + c[0] + c[1] + c[2] + alpha;
+    fits = t <= 65535u && c[0] <= 65535u && c[1] <= 65535u && c[2] <= 65535u;
+    return t;
+}
+
+constexpr int kRcThreads = 256;
+
+__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, uint64_t *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    uint64_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+    return t;
+}
+
+__global__ void __launch_bounds__(kRcThreads) k_rc_init(EncodeLaunch e) {
+    __shared__ uint64_t sh[kRcThreads / 32];
+    const EncPicDesc pd = e.pics[blockIdx.x];
+    uint64_t a = 0;
+    for (uint32_t k = threadIdx.x; k < pd.n_slices; k += kRcThreads) a += e.alpha_bytes[pd.slice_base + k];
+    const uint64_t alpha = block_sum_u64(a, sh);
+    if (threadIdx.x == 0) {
+        // Alpha is lossless and comes on top of the rate; the picture
+        // header and the slice table come out of it (src/encode.rs:686-689).
+        const uint64_t overhead = 8u + 2ull * pd.n_slices;
+        const uint64_t b = pd.budget_in + alpha;
+        EncPicState st{};
+        st.budget = b > overhead ? b - overhead : 0;
+        st.lo = 1;
+        st.hi = 224;
+        st.probe_qi = 224;
+        st.hi_probe = 0;
+        st.fits_at_all = 0;
+        st.uniform = 224;
+        e.state[blockIdx.x] = st;
+    }
+}
+
+__global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step) {
+    __shared__ uint64_t sh[kRcThreads / 32];
+    __shared__ int all_fit;
+    const EncPicDesc pd = e.pics[blockIdx.x];
+    const EncPicState st0 = e.state[blockIdx.x];
+    if (st0.probe_qi == 0) return;
+    if (threadIdx.x == 0) all_fit = 1;
+    __syncthreads();
+    uint64_t sum = 0;
+    bool fit = true;
+    for (uint32_t k = threadIdx.x; k < pd.n_slices; k += kRcThreads) {
+        const uint32_t s = pd.slice_base + k;
+        const uint32_t *c = e.probe_comp + ((uint64_t)step * e.n_slices + s) * 3u;
+        const uint32_t cc[3] = {c[0], c[1], c[2]};
+        bool f;
+        sum += slice_total(pd.header_bytes, cc, e.alpha_bytes[s], f);
+        fit = fit && f;
+    }
+    if (!fit) all_fit = 0;
+    const uint64_t total = block_sum_u64(sum, sh);
+    if (threadIdx.x == 0) {
+        EncPicState st = st0;
+        const bool ok = all_fit && total <= st.budget;
+        if (step == 0) {
+            // totals(224): if even the coarsest quantiser does not fit, it is
+            // used throughout (src/encode.rs:701-713).
+            st.fits_at_all = ok;
+            st.hi_probe = 0;
+            if (!ok) {
+                st.probe_qi = 0;
+                st.uniform = 224;
+            }
+        } else if (ok) {
+            st.hi = st.probe_qi;
+            st.hi_probe = step;
+        } else {
+            st.lo = st.probe_qi + 1;
+        }
+        if (st.fits_at_all) {
+            if (st.lo < st.hi) {
+                st.probe_qi = st.lo + (st.hi - st.lo) / 2;
+            } else {
+                st.probe_qi = 0;
+                st.uniform = st.hi;
+            }
+        }
+        e.state[blockIdx.x] = st;
+    }
+}
+
+// The share-out (src/encode.rs:769-793): one warp per picture walks its
+// slices in order; every lane runs the same recurrence so that the warp can
+// cost a deeper quantiser together when one is needed.
+constexpr int kShareWarps = 4;
+
+__global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
+    const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
+    if (p >= e.n_pics) return;
+    const int lane = threadIdx.x & 31;
+    const EncPicDesc pd = e.pics[p];
+    const EncPicState st = e.state[p];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const uint32_t *used_c = e.probe_comp + (uint64_t)st.hi_probe * e.n_slices * 3u;
+    const uint32_t hb = pd.header_bytes;
+    if (!(st.uniform > 1 && st.fits_at_all)) {
+        for (uint32_t k = lane; k < pd.n_slices; k += 32) {
+            const uint32_t s = pd.slice_base + k;
+            e.final_qi[s] = (uint32_t)st.uniform;
+            for (int c = 0; c < 3; c++) e.final_comp[3ull * s + c] = used_c[3ull * s + c];
+        }
+        return;
+    }
+    uint64_t used_sum = 0, mbs_sum = 0;
+    for (uint32_t k = lane; k < pd.n_slices; k += 32) {
+        const uint32_t s = pd.slice_base + k;
+        const uint32_t cc[3] = {used_c[3ull * s], used_c[3ull * s + 1], used_c[3ull * s + 2]};
+        bool f;
+        used_sum += slice_total(hb, cc, e.alpha_bytes[s], f);
+        mbs_sum += e.slices[s].mbs;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        used_sum += __shfl_xor_sync(0xffffffffu, used_sum, o);
+        mbs_sum += __shfl_xor_sync(0xffffffffu, mbs_sum, o);
+    }
+    uint64_t rem_budget = st.budget, rem_base = used_sum, rem_mbs = mbs_sum;
+    for (uint32_t k0 = 0; k0 < pd.n_slices; k0 += 32) {
+        // Each lane fetches one of the next 32 slices' sizes; the walk then
+        // reads them by shuffles.
+        const uint32_t k = k0 + lane;
+        uint32_t my_mbs = 0, my_alpha = 0, u0 = 0, u1 = 0, u2 = 0, w0 = 0, w1 = 0, w2 = 0;
+        if (k < pd.n_slices) {
+            const uint32_t s = pd.slice_base + k;
+            my_mbs = e.slices[s].mbs;
+            my_alpha = e.alpha_bytes[s];
+            u0 = used_c[3ull * s];
+            u1 = used_c[3ull * s + 1];
+            u2 = used_c[3ull * s + 2];
+            const uint32_t *w = e.win_comp + 3ull * s;
+            w0 = w[0];
+            w1 = w[1];
+            w2 = w[2];
+        }
+        const uint32_t count = min(32u, pd.n_slices - k0);
+        for (uint32_t i = 0; i < count; i++) {
+            const uint32_t s = pd.slice_base + k0 + i;
+            const uint32_t mbs = __shfl_sync(0xffffffffu, my_mbs, i);
+            const uint32_t alpha = __shfl_sync(0xffffffffu, my_alpha, i);
+            uint32_t cur[3] = {__shfl_sync(0xffffffffu, u0, i), __shfl_sync(0xffffffffu, u1, i),
+                               __shfl_sync(0xffffffffu, u2, i)};
+            const uint32_t first[3] = {__shfl_sync(0xffffffffu, w0, i), __shfl_sync(0xffffffffu, w1, i),
+                                       __shfl_sync(0xffffffffu, w2, i)};
+            bool f;
+            const uint64_t base = slice_total(hb, cur, alpha, f);
+            const uint64_t slack = rem_budget - rem_base;
+            const uint64_t allowed = base + slack * mbs / rem_mbs;
+            uint64_t used = base;
+            int32_t qi = st.uniform;
+            while (qi > 1) {
+                const uint32_t stepd = (uint32_t)(st.uniform - qi);
+                uint32_t c3[3];
+                if (stepd == 0) {
+                    c3[0] = first[0];
+                    c3[1] = first[1];
+                    c3[2] = first[2];
+                } else if (stepd < (uint32_t)kWindow) {
+                    const uint32_t *w = e.win_comp + ((uint64_t)stepd * e.n_slices + s) * 3u;
+                    c3[0] = w[0];
+                    c3[1] = w[1];
+                    c3[2] = w[2];
+                } else {
+                    const EncSliceDesc sd = e.slices[s];
+                    for (uint32_t c = 0; c < 3; c++) c3[c] = component_bytes(e, sd, pd, fd, c, (uint32_t)(qi - 1));
+                }
+                bool fits;
+                const uint64_t n = slice_total(hb, c3, alpha, fits);
+                if (!(fits && n <= allowed)) break;
+                qi -= 1;
+                used = n;
+                cur[0] = c3[0];
+                cur[1] = c3[1];
+                cur[2] = c3[2];
+            }
+            if (lane == 0) {
+                e.final_qi[s] = (uint32_t)qi;
+                e.final_comp[3ull * s] = cur[0];
+                e.final_comp[3ull * s + 1] = cur[1];
+                e.final_comp[3ull * s + 2] = cur[2];
+            }
+            rem_budget -= used;
+            rem_base -= base;
+            rem_mbs -= mbs;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- layout
+
+constexpr int kLayoutThreads = 1024;
+
+__device__ __forceinline__ uint64_t warp_incl_scan64(uint64_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Slice offsets within the picture (after its header and table) and the
+// picture's size (src/encode.rs:820-829).
+__global__ void __launch_bounds__(kLayoutThreads) k_layout(EncodeLaunch e) {
+    __shared__ uint64_t warp_sums[kLayoutThreads / 32];
+    __shared__ uint64_t carry;
+    const EncPicDesc pd = e.pics[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 8u + 2ull * pd.n_slices;
+    __syncthreads();
+    for (uint32_t chunk = 0; chunk < pd.n_slices; chunk += kLayoutThreads) {
+        const uint32_t k = chunk + threadIdx.x;
+        uint64_t size = 0;
+        if (k < pd.n_slices) {
+            const uint32_t s = pd.slice_base + k;
+            const uint32_t cc[3] = {e.final_comp[3ull * s], e.final_comp[3ull * s + 1], e.final_comp[3ull * s + 2]};
+            bool f;
+            size = slice_total(pd.header_bytes, cc, e.alpha_bytes[s], f);
+        }
+        const uint64_t incl = warp_incl_scan64(size);
+        if (lane == 31) warp_sums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) warp_sums[lane] = warp_incl_scan64(warp_sums[lane]);
+        __syncthreads();
+        const uint64_t excl = carry + (warp ? warp_sums[warp - 1] : 0u) + incl - size;
+        if (k < pd.n_slices) e.slice_off[pd.slice_base + k] = excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_sums[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) e.state[blockIdx.x].pic_size = carry;
+}
+
+// Picture places and sizes, the frame header and frame_size, the picture
+// headers (src/header.rs:174-199, :292-304). One thread per frame.
+__global__ void k_frame(EncodeLaunch e) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= e.n_frames) return;
+    const EncFrameDesc fd = e.frames[f];
+    uint64_t pos = fd.header_len;
+    for (uint32_t i = 0; i < fd.n_pics; i++) {
+        e.state[fd.first_pic + i].pic_off = pos;
+        pos += e.state[fd.first_pic + i].pic_size;
+    }
+    e.frame_size[f] = pos;
+    const bool over = pos > fd.out_cap;
+    e.frame_status[f] = over ? 1u : 0u;
+    if (over) return;
+    const uint64_t base = fd.out_base * 8u;
+    const uint8_t *h = e.headers + (uint64_t)kHeaderSlot * fd.header_slot;
+    put_field(e.out, base, (uint32_t)pos, 32);  // frame_size
+    for (uint32_t b = 4; b < fd.header_len; b++) put_field(e.out, base + 8ull * b, h[b], 8);
+    for (uint32_t i = 0; i < fd.n_pics; i++) {
+        const EncPicDesc &pd = e.pics[fd.first_pic + i];
+        const EncPicState &st = e.state[fd.first_pic + i];
+        const uint64_t at = base + 8ull * st.pic_off;
+        put_field(e.out, at, 8u << 3, 8);
+        put_field(e.out, at + 8, (uint32_t)st.pic_size, 32);
+        put_field(e.out, at + 40, pd.n_slices <= 65535u ? pd.n_slices : 0u, 16);
+        put_field(e.out, at + 56, (pd.log2_slice_mbs & 3u) << 4, 8);
+    }
+}
+
+// ---------------------------------------------------------------- packing
+
+// Writes one quantised component's codes (src/encode.rs:413-437) from bit
+// `bitpos`: each lane's codeword lengths, scanned across the warp, give its
+// place.
+__device__ void component_write(uint32_t *out, uint64_t bitpos, const float *f, uint32_t n_blocks, const float *inv) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = 64u * n_blocks;
+    const uint32_t shift = 31u - __clz(n_blocks);
+    uint64_t carry_bits = 0;
+    int32_t carry_pos = (int32_t)n_blocks - 1;
+    uint32_t carry_run = 4, carry_level = 1;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t p = base + lane;
+        const uint32_t sidx = p >> shift;
+        const int32_t q = quantise1(f[p], __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
+        uint32_t len = 0;
+        uint64_t cw0 = 0, cw1 = 0;
+        uint32_t l0 = 0, l1 = 0;
+        bool neg = false;
+        if (base == 0) {
+            const int32_t left = __shfl_up_sync(0xffffffffu, q, 1);
+            const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)left);
+            const int32_t prev_diff_raw = __shfl_up_sync(0xffffffffu, diff, 1);
+            if (p < n_blocks) {
+                Codebook cb;
+                uint32_t sym;
+                if (p == 0) {
+                    cb = kFirstDcBook;
+                    sym = signed_to_symbol(q);
+                } else {
+                    const int32_t prev_diff = p == 1 ? 3 : prev_diff_raw;
+                    cb = dc_book(prev_diff);
+                    sym = signed_to_symbol(prev_diff < 0 ? -diff : diff);
+                }
+                cw0 = cb_bits(cb, sym);
+                l0 = cb_len(cb, sym);
+                len = l0;
+            }
+        }
+        const bool nz = q != 0 && p >= n_blocks;
+        const uint32_t mask = __ballot_sync(0xffffffffu, nz);
+        const uint32_t below = mask & ((1u << lane) - 1u);
+        const int src = below ? 31 - __clz(below) : lane;
+        const int32_t prev_pos = below ? (int32_t)(base + src) : carry_pos;
+        const uint32_t run = nz ? (uint32_t)((int32_t)p - prev_pos - 1) : 0u;
+        const uint32_t level = nz ? (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u : 0u;
+        const uint32_t src_run = __shfl_sync(0xffffffffu, run, src);
+        const uint32_t src_level = __shfl_sync(0xffffffffu, level, src);
+        if (nz) {
+            const Codebook rb = run_book(below ? src_run : carry_run);
+            const Codebook lb = level_book(below ? src_level : carry_level);
+            cw0 = cb_bits(rb, run);
+            l0 = cb_len(rb, run);
+            cw1 = cb_bits(lb, level);
+            l1 = cb_len(lb, level);
+            neg = q < 0;
+            len = l0 + l1 + 1u;
+        }
+        uint64_t incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (len) {
+            const uint64_t at = bitpos + carry_bits + incl - len;
+            put_field(out, at, cw0, l0);
+            if (nz) {
+                put_field(out, at + l0, cw1, l1);
+                if (neg) put_field(out, at + l0 + l1, 1u, 1u);
+            }
+        }
+        carry_bits += __shfl_sync(0xffffffffu, incl, 31);
+        if (mask) {
+            const int top = 31 - __clz(mask);
+            carry_pos = (int32_t)(base + top);
+            carry_run = __shfl_sync(0xffffffffu, run, top);
+            carry_level = __shfl_sync(0xffffffffu, level, top);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_pack(EncodeLaunch e) {
+    __shared__ AlphaScratch scratch;
+    const uint32_t s = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    if (e.frame_status[pd.frame]) return;
+    const EncPicState &st = e.state[sd.pic];
+    const uint32_t comp[3] = {e.final_comp[3ull * s], e.final_comp[3ull * s + 1], e.final_comp[3ull * s + 2]};
+    const uint32_t qi = e.final_qi[s];
+    const uint64_t slice_bit = 8ull * (fd.out_base + st.pic_off + e.slice_off[s]);
+    const uint32_t hb = pd.header_bytes;
+    if (warp < 3) {
+        uint64_t at = slice_bit + 8ull * hb;
+        for (int c = 0; c < warp; c++) at += 8ull * comp[c];
+        uint32_t nb, off;
+        comp_layout(fd, sd.mbs, (uint32_t)warp, nb, off);
+        component_write(e.out, at, e.coef + sd.coef + off, nb, quant_table(e, pd, qi, (uint32_t)warp));
+    } else {
+        if (lane == 0) {
+            // Slice header: size << 3, quantization_index, the component
+            // sizes (the Cr size only with alpha); the table entry.
+            bool f;
+            const uint64_t total = slice_total(hb, comp, e.alpha_bytes[s], f);
+            put_field(e.out, slice_bit, hb << 3, 8);
+            put_field(e.out, slice_bit + 8, qi, 8);
+            put_field(e.out, slice_bit + 16, comp[0] & 0xFFFFu, 16);
+            put_field(e.out, slice_bit + 32, comp[1] & 0xFFFFu, 16);
+            if (hb == 8) put_field(e.out, slice_bit + 48, comp[2] & 0xFFFFu, 16);
+            const uint64_t table_bit = 8ull * (fd.out_base + st.pic_off + 8u + 2ull * (s - pd.slice_base));
+            put_field(e.out, table_bit, (uint32_t)(total & 0xFFFFu), 16);
+        }
+        if (fd.alpha_bits) {
+            const uint64_t at = slice_bit + 8ull * ((uint64_t)hb + comp[0] + comp[1] + comp[2]);
+            alpha_write(e, sd, pd, fd, scratch, at);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    k_fdct<<<e.n_slices, kFdctThreads, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_alpha_size(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    if (!e.any_alpha) return cudaMemsetAsync(e.alpha_bytes, 0, 4ull * e.n_slices, s);
+    k_alpha_size<<<(e.n_slices + kAlphaWarps - 1) / kAlphaWarps, 32 * kAlphaWarps, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_pics) return cudaSuccess;
+    k_rc_init<<<e.n_pics, kRcThreads, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    const uint32_t items = 3u * e.n_slices;
+    k_cost<<<(items + kCostWarps - 1) / kCostWarps, 32 * kCostWarps, 0, s>>>(e, step);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s) {
+    if (!e.n_pics) return cudaSuccess;
+    k_rc_step<<<e.n_pics, kRcThreads, 0, s>>>(e, step);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cost_window(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    const uint32_t items = 3u * kWindow * e.n_slices;
+    k_cost_window<<<(items + kCostWarps - 1) / kCostWarps, 32 * kCostWarps, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_pics) return cudaSuccess;
+    k_shareout<<<(e.n_pics + kShareWarps - 1) / kShareWarps, 32 * kShareWarps, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s) {
+    if (e.n_pics) k_layout<<<e.n_pics, kLayoutThreads, 0, s>>>(e);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess || !e.n_frames) return err;
+    k_frame<<<(e.n_frames + 127) / 128, 128, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    k_pack<<<e.n_slices, 128, 0, s>>>(e);
+    return cudaGetLastError();
+}
+
+cudaError_t configure_encode_kernels() {
+    uint8_t sc[2][64];
+    for (int i = 0; i < 64; i++) {
+        sc[0][i] = kProgressiveScan[i];
+        sc[1][i] = kInterlacedScan[i];
+    }
+    return cudaMemcpyToSymbol(c_enc_scan, sc, sizeof sc);
+}
+
+}  // namespace prores

@@ -1,0 +1,103 @@
+// encode_types.h -- descriptors and launch parameters of the encode kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace prores {
+
+// Bisection steps after the probe at 224: the interval [1, 224] halves
+// (rounding up) to one value in 8 steps (src/encode.rs:700-713).
+constexpr int kProbeSteps = 9;
+// Finer quantisers costed in one pass before the share-out; deeper ones are
+// costed by the share-out itself.
+constexpr int kWindow = 4;
+// Bytes per frame-header template: 8 + a frame_header() of at most 148.
+constexpr uint32_t kHeaderSlot = 160;
+
+struct EncFrameDesc {
+    uint64_t in_off[3];     // sample offsets of Y', Cb, Cr in the input plane buffer
+    uint64_t alpha_in_off;  // sample offset of the alpha plane in the input alpha buffer
+    uint64_t out_base;      // byte offset of the frame's region in the output buffer (4-aligned)
+    uint64_t out_cap;       // bytes available there
+    uint64_t rescale_m;     // input depth -> coded alpha bits (src/encode.rs:850-852)
+    uint32_t width, height;
+    uint32_t plane_w[3];
+    uint32_t chroma;      // 2 or 3
+    uint32_t bit_depth;   // input depth, 8-16
+    uint32_t alpha_bits;  // coded alpha: 0, 8 or 16
+    uint32_t rescale_identity;
+    uint32_t header_len;  // frame_size + 'icpf' + frame_header() bytes
+    uint32_t header_slot; // index of the frame's header template (kHeaderSlot bytes each)
+    uint32_t first_pic, n_pics;
+    float in_scale;  // 512 / 2^b (src/encode.rs:524-525)
+};
+
+struct EncPicDesc {
+    uint64_t coef_base;  // first f32 coefficient of the picture
+    uint64_t budget_in;  // the picture's share of the target (src/encode.rs:272)
+    uint32_t slice_base, n_slices, slices_per_row, width_in_mb, height_in_mb;
+    uint32_t log2_slice_mbs;
+    uint32_t frame;
+    uint32_t height, first_row, row_step;
+    uint32_t quant;         // index of the picture's quantiser table set
+    uint32_t header_bytes;  // slice header: 6, or 8 with alpha
+    uint32_t interlaced_scan;
+};
+
+struct EncSliceDesc {
+    uint64_t coef;  // first coefficient (scanned order, Y' then Cb then Cr)
+    uint32_t pic;
+    uint16_t mb_x, mb_y;
+    uint32_t mbs;
+};
+
+// Rate-control state of one picture (src/encode.rs:685-794).
+struct EncPicState {
+    uint64_t budget;     // bytes for the slices
+    uint64_t pic_size;   // picture_size once coded
+    uint64_t pic_off;    // byte offset of the picture in its frame
+    int32_t lo, hi;      // bisection interval
+    int32_t probe_qi;    // quantiser of the pass in flight (0: none)
+    int32_t hi_probe;    // the probe step whose sizes are at `hi`
+    int32_t fits_at_all;
+    int32_t uniform;
+    int32_t pad[2];
+};
+
+struct EncodeLaunch {
+    const uint16_t *in;        // input planes
+    const uint16_t *alpha_in;  // input alpha planes
+    const EncFrameDesc *frames;
+    const EncPicDesc *pics;
+    const EncSliceDesc *slices;
+    EncPicState *state;
+    float *coef;           // transformed slices, scanned order
+    const float *quant;    // [set][225 qi][2][64] 8 / (W qScale) at scanned positions
+    const float *basis;    // T[x][u]
+    uint32_t *alpha_bytes; // per slice
+    uint32_t *probe_comp;  // [kProbeSteps][slice][3] component bytes
+    uint32_t *win_comp;    // [kWindow][slice][3]
+    uint32_t *final_comp;  // [slice][3]
+    uint32_t *final_qi;    // [slice]
+    uint64_t *slice_off;   // [slice] byte offset of the slice in its frame
+    uint32_t *out;         // output buffer (zeroed before packing), big-endian bit order
+    const uint8_t *headers;  // frame header templates
+    uint32_t *frame_status;  // per frame: 0, or 1 when the frame outgrew its region
+    uint64_t *frame_size;    // per frame
+    uint32_t n_frames, n_pics, n_slices;
+    int any_alpha;
+};
+
+cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_alpha_size(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s);
+cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s);
+cudaError_t launch_cost_window(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s);
+
+}  // namespace prores

@@ -1,0 +1,763 @@
+// engine.cpp -- contexts, workspaces and the decode side of the batch engine.
+//
+// A batch of frames becomes one flat list of frames, pictures and slices:
+// the host parses each frame's header and picture headers (src/header.rs),
+// lays the frames' bytes end to end in one device buffer, and the kernels do
+// everything per slice. Errors keep the crate's precedence: a frame-header
+// failure first; then, picture by picture, a picture-header or slice-table
+// failure, a slice that runs past picture_size, and the first failing slice
+// component in picture order (src/decode.rs:85-104, :188-290).
+
+#include "engine.h"
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "codec_tables.h"
+
+namespace prores {
+
+cudaError_t configure_decode_kernels();
+cudaError_t configure_encode_kernels();
+
+static thread_local std::string g_last_error;
+
+static thread_local std::vector<std::string> g_batch_errors;
+
+void set_last_error(const Status &s) { g_last_error = display(s); }
+
+void set_batch_errors(const std::vector<Status> &errs) {
+    g_batch_errors.assign(errs.size(), std::string());
+    for (size_t i = 0; i < errs.size(); i++)
+        if (errs[i]) g_batch_errors[i] = display(errs[i]);
+}
+
+Status cuda_status(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return Status();
+    return make_status(PRORES_DEVICE, strf("%s: %s", what, cudaGetErrorString(e)));
+}
+
+#define PR_CUDA(expr, what)                                   \
+    do {                                                      \
+        Status st_ = cuda_status((expr), what);               \
+        if (st_) return st_;                                  \
+    } while (0)
+
+cudaError_t DeviceBuf::reserve(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+
+DeviceBuf::~DeviceBuf() {
+    if (p) cudaFree(p);
+}
+
+cudaError_t PinnedBuf::reserve(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 8 + 4096;
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+
+PinnedBuf::~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+}
+
+Workspace::~Workspace() {
+    if (stream) cudaStreamDestroy(stream);
+}
+
+std::unique_ptr<Workspace> Context::acquire() {
+    {
+        std::lock_guard<std::mutex> g(m);
+        if (!free_ws.empty()) {
+            auto ws = std::move(free_ws.back());
+            free_ws.pop_back();
+            return ws;
+        }
+    }
+    auto ws = std::make_unique<Workspace>();
+    ws->device = device;
+    cudaSetDevice(device);
+    if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    return ws;
+}
+
+void Context::release(std::unique_ptr<Workspace> ws) {
+    if (!ws) return;
+    std::lock_guard<std::mutex> g(m);
+    free_ws.push_back(std::move(ws));
+}
+
+Context::~Context() {
+    cudaSetDevice(device);
+    free_ws.clear();
+    if (tables.run_decode) cudaFree(tables.run_decode);
+    if (tables.level_decode) cudaFree(tables.level_decode);
+    if (tables.basis) cudaFree(tables.basis);
+}
+
+Status record_kernel(KernelTimes *kt, const char *name, cudaStream_t s) {
+    if (!kt || !kt->enabled) return Status();
+    cudaEvent_t e;
+    PR_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    PR_CUDA(cudaEventRecord(e, s), "cudaEventRecord");
+    kt->events.push_back(e);
+    kt->names.push_back(name);
+    return Status();
+}
+
+// ------------------------------------------------------------------ decode
+
+static const char *device_message(int code) {
+    switch (code) {
+    case DE_PAST_END: return "a codeword runs past the end of its data";
+    case DE_PREFIX: return "a variable-length code's prefix is too long";
+    case DE_RANGE: return "a variable-length code's value is out of range";
+    case DE_DC_OVERFLOW: return "a DC coefficient overflows";
+    case DE_RUN_PAST_END: return "a run passes the end of the coefficient array";
+    case DE_ALPHA_RUN: return "an alpha run passes the end of the slice";
+    case DE_SLICE_SHORT: return "a slice is shorter than its header";
+    case DE_COMP_SIZES: return "slice component sizes exceed the slice";
+    }
+    return "unknown slice failure";
+}
+
+static Status slot_status(int code, int aux) {
+    if (code == DE_SLICE_HDR_SIZE) return make_status(PRORES_INVALID, strf("slice_header_size %d is out of range", aux));
+    if (code == DE_QINDEX) return make_status(PRORES_INVALID, strf("quantization_index %d is reserved", aux));
+    return make_status(PRORES_INVALID, device_message(code));
+}
+
+static uint32_t add_weights(std::vector<uint8_t> &w, const FrameHeader &h) {
+    uint8_t set[128];
+    h.luma_weights(set);
+    h.chroma_weights(set + 64);
+    for (size_t i = 0; i + 128 <= w.size(); i += 128)
+        if (memcmp(&w[i], set, 128) == 0) return (uint32_t)(i / 128);
+    w.insert(w.end(), set, set + 128);
+    return (uint32_t)(w.size() / 128 - 1);
+}
+
+Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan) {
+    plan = DecodePlan();
+    plan.frames.resize(n);
+    size_t bits_pos = 0;
+    const uint8_t *prev_end = nullptr;
+    for (int i = 0; i < n; i++) {
+        DecodeFrame &f = plan.frames[i];
+        // The frame's bytes go after the previous frame's; host-adjacent
+        // buffers go over in one copy.
+        f.bits_off = bits_pos;
+        if (in[i].len) {
+            if (!plan.copies.empty() && prev_end == in[i].data)
+                plan.copies.back().len += in[i].len;
+            else
+                plan.copies.push_back({in[i].data, bits_pos, in[i].len});
+            prev_end = in[i].data + in[i].len;
+            bits_pos += in[i].len;
+        }
+        if (out_depth != 0 && (out_depth < 8 || out_depth > 16)) {
+            f.err = make_status(PRORES_CONFIG, strf("output bit depth %u is outside 8\xe2\x80\x93" "16", out_depth));
+            continue;
+        }
+        if ((f.err = parse_frame_header(in[i].data, in[i].len, &f.hdr))) continue;
+        if ((f.err = check_plausible_size(f.hdr))) continue;
+        const FrameHeader &h = f.hdr;
+        f.depth = out_depth ? out_depth : (h.chroma == PRORES_CHROMA_422 ? 10u : 12u);
+        FrameDesc fd{};
+        size_t off[3];
+        f.samples = frame_layout(h.width, h.height, h.chroma, off, fd.plane_w);
+        f.plane_off = plan.planes_total;
+        plan.planes_total += f.samples;
+        for (int c = 0; c < 3; c++) fd.plane_off[c] = f.plane_off + off[c];
+        if (h.alpha) {
+            f.alpha_samples = (size_t)h.width * h.height;
+            f.alpha_off = plan.alpha_total;
+            plan.alpha_total += f.alpha_samples;
+        }
+        fd.alpha_off = f.alpha_off;
+        fd.width = h.width;
+        fd.height = h.height;
+        fd.chroma = (uint32_t)h.chroma;
+        fd.alpha_bits = h.alpha_bits();
+        fd.bit_depth = f.depth;
+        fd.weights = add_weights(plan.weights, h);
+        if (fd.alpha_bits) {
+            fd.rescale_m = rescale_multiplier(fd.alpha_bits, f.depth);
+            fd.rescale_identity = fd.alpha_bits == f.depth;
+        }
+        // §7.5.1: s = floor(v 2^b / 512 + 2^(b-1) + 1/2) in [0, 2^b - 1].
+        fd.out_scale = (float)(1u << f.depth) / 512.0f;
+        fd.out_bias = (float)(1u << (f.depth - 1)) + 0.5f;
+        fd.out_max = (float)((1u << f.depth) - 1);
+        f.desc = (int)plan.fdesc.size();
+        plan.fdesc.push_back(fd);
+
+        // Pictures: headers and slice tables are checked here; what fails is
+        // reported after the pictures before it are decoded.
+        const uint32_t cpm = h.chroma == PRORES_CHROMA_422 ? 2u : 4u;
+        const uint32_t width_in_mb = (h.width + 15u) / 16u;
+        size_t pos = 8 + (size_t)h.header_size;
+        const size_t flen = h.frame_size;
+        f.first_pic = (uint32_t)plan.pdesc.size();
+        for (uint32_t index = 0; index < h.picture_count(); index++) {
+            if (pos > flen) {
+                f.late = make_status(PRORES_INVALID, "a picture starts past the end of the frame");
+                break;
+            }
+            PictureHeader ph;
+            if ((f.late = parse_picture_header(in[i].data + pos, flen - pos, &ph))) break;
+            const uint32_t height = h.picture_height(index);
+            const uint32_t height_in_mb = (height + 15u) / 16u;
+            const uint32_t spr = slices_per_row(width_in_mb, ph.log2_slice_mbs);
+            const uint64_t n_slices = (uint64_t)spr * height_in_mb;
+            if ((uint64_t)ph.header_size + 2 * n_slices > ph.picture_size) {
+                f.late = make_status(PRORES_INVALID, "the slice table runs past picture_size");
+                break;
+            }
+            PicDesc p{};
+            p.off = f.bits_off + pos;
+            p.coef_base = plan.coef_total;
+            p.header_size = ph.header_size;
+            p.picture_size = ph.picture_size;
+            p.n_slices = (uint32_t)n_slices;
+            p.slices_per_row = spr;
+            p.width_in_mb = width_in_mb;
+            p.height_in_mb = height_in_mb;
+            p.log2_slice_mbs = ph.log2_slice_mbs;
+            p.slice_base = plan.n_slices;
+            p.frame = (uint32_t)f.desc;
+            p.height = height;
+            h.picture_rows(index, &p.first_row, &p.row_step);
+            p.interlaced_scan = h.interlace != 0;
+            plan.pdesc.push_back(p);
+            plan.n_slices += (uint32_t)n_slices;
+            plan.coef_total += (size_t)width_in_mb * height_in_mb * 64u * (4u + 2u * cpm);
+            f.n_pics++;
+            pos += ph.picture_size;
+        }
+    }
+    plan.bits_total = bits_pos;
+    return Status();
+}
+
+Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s) {
+    (void)in;
+    for (const auto &c : plan.copies)
+        PR_CUDA(cudaMemcpyAsync(ws.bits.as<uint8_t>() + c.dst, c.src, c.len, cudaMemcpyHostToDevice, s),
+                "bitstream upload");
+    return Status();
+}
+
+Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s) {
+    (void)ctx;
+    // 64 bytes of zero padding after the bitstreams: the readers fetch the
+    // aligned word after the one they are in.
+    PR_CUDA(ws.bits.reserve(plan.bits_total + 64), "cudaMalloc bitstream");
+    PR_CUDA(cudaMemsetAsync(ws.bits.as<uint8_t>() + plan.bits_total, 0, 64, s), "memset");
+    PR_CUDA(ws.frames.reserve(sizeof(FrameDesc) * (plan.fdesc.size() + 1)), "cudaMalloc");
+    PR_CUDA(ws.pics.reserve(sizeof(PicDesc) * (plan.pdesc.size() + 1)), "cudaMalloc");
+    PR_CUDA(ws.slices.reserve(sizeof(SliceDesc) * (plan.n_slices + 1)), "cudaMalloc");
+    PR_CUDA(ws.slot_status.reserve(sizeof(int2) * 4 * ((size_t)plan.n_slices + 1)), "cudaMalloc");
+    PR_CUDA(ws.pic_status.reserve(sizeof(PicStatus) * (plan.pdesc.size() + 1)), "cudaMalloc");
+    PR_CUDA(ws.planes.reserve(2 * (plan.planes_total + 8)), "cudaMalloc planes");
+    PR_CUDA(ws.alpha.reserve(2 * (plan.alpha_total + 8)), "cudaMalloc alpha");
+    PR_CUDA(ws.weights.reserve(plan.weights.size() + 128), "cudaMalloc");
+    PR_CUDA(ws.counter.reserve(64), "cudaMalloc");
+    const size_t coef_bytes = 4 * (plan.coef_total + 64);
+    if (coef_bytes > ws.coef.cap || !ws.coef.p) {
+        PR_CUDA(ws.coef.reserve(coef_bytes), "cudaMalloc coefficient scratch");
+        ws.coef_clean = false;
+    }
+    if (!ws.coef_clean) {
+        PR_CUDA(cudaMemsetAsync(ws.coef.p, 0, ws.coef.cap, s), "memset scratch");
+        ws.coef_clean = true;
+    }
+    if (!plan.fdesc.empty())
+        PR_CUDA(cudaMemcpyAsync(ws.frames.p, plan.fdesc.data(), sizeof(FrameDesc) * plan.fdesc.size(),
+                                cudaMemcpyHostToDevice, s),
+                "upload");
+    if (!plan.pdesc.empty())
+        PR_CUDA(cudaMemcpyAsync(ws.pics.p, plan.pdesc.data(), sizeof(PicDesc) * plan.pdesc.size(),
+                                cudaMemcpyHostToDevice, s),
+                "upload");
+    if (!plan.weights.empty())
+        PR_CUDA(cudaMemcpyAsync(ws.weights.p, plan.weights.data(), plan.weights.size(), cudaMemcpyHostToDevice, s),
+                "upload");
+    // Pageable descriptor vectors: the copies above are staged by the
+    // driver before returning, so the plan may change afterwards.
+    return Status();
+}
+
+DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan &plan) {
+    DecodeLaunch d{};
+    d.bits = ws.bits.as<uint8_t>();
+    d.bits_len = plan.bits_total;
+    d.frames = ws.frames.as<FrameDesc>();
+    d.pics = ws.pics.as<PicDesc>();
+    d.slices = ws.slices.as<SliceDesc>();
+    d.slot_status = ws.slot_status.as<int2>();
+    d.pic_status = ws.pic_status.as<PicStatus>();
+    d.coef = ws.coef.as<int32_t>();
+    d.planes = ws.planes.as<uint16_t>();
+    d.alpha = ws.alpha.as<uint16_t>();
+    d.weights = ws.weights.as<uint8_t>();
+    d.work_counter = ws.counter.as<unsigned int>();
+    d.n_frames = (uint32_t)plan.fdesc.size();
+    d.n_pics = (uint32_t)plan.pdesc.size();
+    d.n_slices = plan.n_slices;
+    d.tables = ctx.tables;
+    return d;
+}
+
+Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s, KernelTimes *kt) {
+    const DecodeLaunch d = decode_launch_params(ctx, ws, plan);
+    PR_CUDA(cudaMemsetAsync(d.work_counter, 0, sizeof(unsigned int), s), "memset");
+    Status st;
+    if ((st = record_kernel(kt, "start", s))) return st;
+    PR_CUDA(launch_locate(d, s), "k_locate");
+    if ((st = record_kernel(kt, "k_locate", s))) return st;
+    PR_CUDA(launch_entropy(d, ctx.entropy_grid, s), "k_entropy");
+    if ((st = record_kernel(kt, "k_entropy", s))) return st;
+    PR_CUDA(launch_idct(d, s), "k_idct");
+    if ((st = record_kernel(kt, "k_idct", s))) return st;
+    PR_CUDA(launch_status(d, s), "k_status");
+    if ((st = record_kernel(kt, "k_status", s))) return st;
+    return Status();
+}
+
+Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
+                    Status *first_err) {
+    std::vector<PicStatus> ps(plan.pdesc.size());
+    if (!ps.empty())
+        PR_CUDA(cudaMemcpyAsync(ps.data(), ws.pic_status.p, sizeof(PicStatus) * ps.size(), cudaMemcpyDeviceToHost, s),
+                "status download");
+    // Planes straight into the caller's buffers (one copy per run of
+    // host-adjacent frames).
+    struct Run {
+        uint16_t *dst;
+        size_t src, len;
+        bool alpha;
+    };
+    std::vector<Run> runs;
+    const int n = (int)plan.frames.size();
+    for (int i = 0; i < n; i++) {
+        const DecodeFrame &f = plan.frames[i];
+        prores_frame &o = out[i];
+        if (f.err) continue;
+        if (!o.data) {
+            o.data = static_cast<uint16_t *>(malloc(2 * (f.samples ? f.samples : 1)));
+            o.data_len = f.samples;
+            if (f.alpha_samples) {
+                o.alpha = static_cast<uint16_t *>(malloc(2 * f.alpha_samples));
+                o.alpha_len = f.alpha_samples;
+            } else {
+                o.alpha = nullptr;
+                o.alpha_len = 0;
+            }
+            if (!o.data || (f.alpha_samples && !o.alpha)) return make_status(PRORES_DEVICE, "host allocation failed");
+        } else if (o.data_len < f.samples || (f.alpha_samples && (!o.alpha || o.alpha_len < f.alpha_samples))) {
+            return make_status(PRORES_CONFIG, "an output buffer is smaller than its frame");
+        }
+        const auto add = [&](uint16_t *dst, size_t src, size_t len, bool alpha) {
+            if (!len) return;
+            if (!runs.empty() && runs.back().alpha == alpha && runs.back().dst + runs.back().len == dst &&
+                runs.back().src + runs.back().len == src)
+                runs.back().len += len;
+            else
+                runs.push_back({dst, src, len, alpha});
+        };
+        add(o.data, f.plane_off, f.samples, false);
+        if (f.alpha_samples) add(o.alpha, f.alpha_off, f.alpha_samples, true);
+    }
+    for (const Run &r : runs) {
+        const uint16_t *src = (r.alpha ? ws.alpha.as<uint16_t>() : ws.planes.as<uint16_t>()) + r.src;
+        PR_CUDA(cudaMemcpyAsync(r.dst, src, 2 * r.len, cudaMemcpyDeviceToHost, s), "plane download");
+    }
+    PR_CUDA(cudaStreamSynchronize(s), "decode");
+    std::vector<Status> errs(n);
+    for (int i = 0; i < n; i++) {
+        const DecodeFrame &f = plan.frames[i];
+        prores_frame &o = out[i];
+        Status st = f.err;
+        if (!st) {
+            const FrameHeader &h = f.hdr;
+            o.width = h.width;
+            o.height = h.height;
+            o.bit_depth = f.depth;
+            o.chroma = h.chroma;
+            o.interlace = h.interlace;
+            o.aspect_ratio = h.aspect_ratio;
+            o.frame_rate_code = h.frame_rate_code;
+            o.color_primaries = h.color_primaries;
+            o.transfer_characteristic = h.transfer_characteristic;
+            o.matrix_coefficients = h.matrix_coefficients;
+            for (uint32_t p = 0; p < f.n_pics && !st; p++) {
+                const PicStatus &q = ps[f.first_pic + p];
+                if (q.locate_slice >= 0)
+                    st = make_status(PRORES_INVALID, "a slice runs past picture_size");
+                else if (q.slot >= 0)
+                    st = slot_status(q.code, q.aux);
+            }
+            if (!st && f.late) st = f.late;
+        }
+        status[i] = st.code;
+        errs[i] = st;
+        if (st && first_err && !*first_err) *first_err = st;
+    }
+    set_batch_errors(errs);
+    return Status();
+}
+
+}  // namespace prores
+
+// ====================================================================== C ABI
+
+using namespace prores;
+
+static int fail(const Status &s) {
+    set_last_error(s);
+    return s.code;
+}
+
+static int fail_or_ok(const Status &s) { return s ? fail(s) : PRORES_OK; }
+
+static Status make_tables(Context &c) {
+    std::vector<uint16_t> run(kRunTableWords), level(kLevelTableWords);
+    build_decode_table(run_book, 16, run.data());
+    build_decode_table(level_book, 9, level.data());
+    // T[x][u] = C(u)/2 cos((2x+1) u pi / 16), computed in double and rounded
+    // once to single precision (the crate's src/dct.rs:11-25).
+    float basis[64];
+    for (int x = 0; x < 8; x++)
+        for (int u = 0; u < 8; u++) {
+            const double cu = u == 0 ? 0.70710678118654752440 : 1.0;
+            const double a = (double)((2 * x + 1) * u) * 3.14159265358979323846 / 16.0;
+            basis[8 * x + u] = (float)(cu / 2.0 * cos(a));
+        }
+    PR_CUDA(cudaMalloc(&c.tables.run_decode, run.size() * 2), "cudaMalloc");
+    PR_CUDA(cudaMalloc(&c.tables.level_decode, level.size() * 2), "cudaMalloc");
+    PR_CUDA(cudaMalloc(&c.tables.basis, sizeof basis), "cudaMalloc");
+    PR_CUDA(cudaMemcpy(c.tables.run_decode, run.data(), run.size() * 2, cudaMemcpyHostToDevice), "upload");
+    PR_CUDA(cudaMemcpy(c.tables.level_decode, level.data(), level.size() * 2, cudaMemcpyHostToDevice), "upload");
+    PR_CUDA(cudaMemcpy(c.tables.basis, basis, sizeof basis, cudaMemcpyHostToDevice), "upload");
+    return Status();
+}
+
+static bool profiling_requested() {
+    const char *v = getenv("PRORES_PROFILE_KERNELS");
+    return v && v[0] && v[0] != '0';
+}
+
+extern "C" {
+
+prores_ctx *prores_create(int device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        fail(make_status(PRORES_DEVICE, "no such CUDA device"));
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        fail(make_status(PRORES_DEVICE, "this library is built for sm_100 (B200) devices"));
+        return nullptr;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        fail(make_status(PRORES_DEVICE, "cudaSetDevice failed"));
+        return nullptr;
+    }
+    auto *ctx = new prores_ctx();
+    ctx->impl.device = device;
+    ctx->impl.sm_count = prop.multiProcessorCount;
+    Status st = make_tables(ctx->impl);
+    if (!st) st = cuda_status(configure_decode_kernels(), "configure decode kernels");
+    if (!st) st = cuda_status(configure_encode_kernels(), "configure encode kernels");
+    if (st) {
+        fail(st);
+        delete ctx;
+        return nullptr;
+    }
+    ctx->impl.entropy_grid = entropy_grid(device);
+    return ctx;
+}
+
+void prores_destroy(prores_ctx *ctx) { delete ctx; }
+
+const char *prores_last_error(void) { return g_last_error.c_str(); }
+
+const char *prores_batch_error(int i) {
+    if (i < 0 || (size_t)i >= g_batch_errors.size()) return "";
+    return g_batch_errors[i].c_str();
+}
+
+int prores_probe(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info) {
+    if (out_bit_depth != 0 && (out_bit_depth < 8 || out_bit_depth > 16))
+        return fail(make_status(PRORES_CONFIG, strf("output bit depth %u is outside 8\xe2\x80\x93" "16", out_bit_depth)));
+    FrameHeader h;
+    Status st = parse_frame_header(data, len, &h);
+    if (!st) st = check_plausible_size(h);
+    if (st) return fail(st);
+    memset(info, 0, sizeof *info);
+    info->width = h.width;
+    info->height = h.height;
+    info->bit_depth = out_bit_depth ? out_bit_depth : (h.chroma == PRORES_CHROMA_422 ? 10u : 12u);
+    info->chroma = h.chroma;
+    info->interlace = h.interlace;
+    info->aspect_ratio = h.aspect_ratio;
+    info->frame_rate_code = h.frame_rate_code;
+    info->color_primaries = h.color_primaries;
+    info->transfer_characteristic = h.transfer_characteristic;
+    info->matrix_coefficients = h.matrix_coefficients;
+    size_t off[3];
+    uint32_t w[3];
+    info->data_len = frame_layout(h.width, h.height, h.chroma, off, w);
+    info->alpha_len = h.alpha ? (size_t)h.width * h.height : 0;
+    return PRORES_OK;
+}
+
+int prores_parse_frame_header(const uint8_t *data, size_t len, prores_frame_header *out) {
+    FrameHeader h;
+    Status st = parse_frame_header(data, len, &h);
+    if (st) return fail(st);
+    memset(out, 0, sizeof *out);
+    out->frame_size = h.frame_size;
+    out->header_size = h.header_size;
+    out->bitstream_version = h.bitstream_version;
+    memcpy(out->encoder_identifier, h.encoder_identifier, 4);
+    out->width = h.width;
+    out->height = h.height;
+    out->chroma = h.chroma;
+    out->interlace = h.interlace;
+    out->alpha = h.alpha;
+    out->aspect_ratio = h.aspect_ratio;
+    out->frame_rate_code = h.frame_rate_code;
+    out->color_primaries = h.color_primaries;
+    out->transfer_characteristic = h.transfer_characteristic;
+    out->matrix_coefficients = h.matrix_coefficients;
+    out->has_luma_matrix = h.has_luma;
+    out->has_chroma_matrix = h.has_chroma;
+    memcpy(out->luma_matrix, h.luma_matrix, 64);
+    memcpy(out->chroma_matrix, h.chroma_matrix, 64);
+    return PRORES_OK;
+}
+
+int prores_decode_batch(prores_ctx *ctx, const prores_buf *in, int n, uint32_t out_bit_depth, prores_frame *out,
+                        int *status) {
+    if (!ctx || n < 0) return fail(make_status(PRORES_CONFIG, "no context"));
+    cudaSetDevice(ctx->impl.device);
+    DecodePlan plan;
+    Status st = plan_decode(in, n, out_bit_depth, plan);
+    if (st) return fail(st);
+    auto ws = ctx->impl.acquire();
+    if (!ws) return fail(make_status(PRORES_DEVICE, "no stream"));
+    cudaStream_t s = ws->stream;
+    st = upload_decode(ctx->impl, *ws, plan, s);
+    if (!st) st = upload_decode_bits(*ws, plan, in, s);
+    if (!st) st = enqueue_decode(ctx->impl, *ws, plan, s, nullptr);
+    Status first;
+    if (!st) st = fetch_decode(*ws, plan, s, out, status, &first);
+    if (st) {
+        cudaStreamSynchronize(s);
+        ws->coef_clean = false;
+        ctx->impl.release(std::move(ws));
+        return fail(st);
+    }
+    ctx->impl.release(std::move(ws));
+    if (first) set_last_error(first);
+    return PRORES_OK;
+}
+
+int prores_decode(prores_ctx *ctx, const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *out) {
+    prores_buf b{data, len};
+    int status = PRORES_OK;
+    int r = prores_decode_batch(ctx, &b, 1, out_bit_depth, out, &status);
+    if (r != PRORES_OK) return r;
+    return status;
+}
+
+void prores_frame_free(prores_frame *f) {
+    if (!f) return;
+    free(f->data);
+    free(f->alpha);
+    f->data = nullptr;
+    f->alpha = nullptr;
+    f->data_len = f->alpha_len = 0;
+}
+
+void prores_buffer_free(void *p) { free(p); }
+
+size_t prores_target_frame_bytes(int32_t profile, uint32_t width, uint32_t height) {
+    if (profile < 0 || profile > 5) return 0;
+    return target_frame_bytes(profile, width, height);
+}
+
+void prores_config_default(prores_config *cfg, int32_t profile) {
+    memset(cfg, 0, sizeof *cfg);
+    cfg->profile = profile;
+    cfg->log2_slice_mbs = 3;
+    cfg->alpha = PRORES_ALPHA_16;
+    cfg->target_frame_bytes = -1;
+    memcpy(cfg->encoder_identifier, "rivt", 4);
+}
+
+// ---- resident decode jobs
+
+int prores_decode_job_create(prores_ctx *ctx, const prores_buf *in, int n, uint32_t out_bit_depth,
+                             prores_decode_job **job) {
+    if (!ctx || n < 0) return fail(make_status(PRORES_CONFIG, "no context"));
+    cudaSetDevice(ctx->impl.device);
+    auto *j = new prores_decode_job();
+    j->ctx = ctx;
+    j->kt.enabled = profiling_requested();
+    Status st = plan_decode(in, n, out_bit_depth, j->plan);
+    if (!st) {
+        j->ws = ctx->impl.acquire();
+        if (!j->ws) st = make_status(PRORES_DEVICE, "no stream");
+    }
+    if (!st) st = upload_decode(ctx->impl, *j->ws, j->plan, j->ws->stream);
+    if (!st) st = upload_decode_bits(*j->ws, j->plan, in, j->ws->stream);
+    if (!st) st = cuda_status(cudaStreamSynchronize(j->ws->stream), "upload");
+    if (st) {
+        prores_decode_job_destroy(j);
+        return fail(st);
+    }
+    *job = j;
+    return PRORES_OK;
+}
+
+int prores_decode_job_upload(prores_decode_job *job, const prores_buf *in, int n, void *stream) {
+    if ((size_t)n != job->plan.frames.size()) return fail(make_status(PRORES_CONFIG, "a job's batch size is fixed"));
+    cudaSetDevice(job->ctx->impl.device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
+    size_t pos = 0;
+    for (int i = 0; i < n; i++) {
+        if (in[i].len != (i + 1 < n ? job->plan.frames[i + 1].bits_off : job->plan.bits_total) - job->plan.frames[i].bits_off)
+            return fail(make_status(PRORES_CONFIG, "a job's frame sizes are fixed"));
+        (void)pos;
+    }
+    // Same sizes, same places: one copy per host-adjacent run.
+    const uint8_t *prev_end = nullptr;
+    size_t run_dst = 0, run_len = 0;
+    const uint8_t *run_src = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!in[i].len) continue;
+        if (run_src && prev_end == in[i].data) {
+            run_len += in[i].len;
+        } else {
+            if (run_src) {
+                Status st = cuda_status(cudaMemcpyAsync(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len,
+                                                        cudaMemcpyHostToDevice, s),
+                                        "bitstream upload");
+                if (st) return fail(st);
+            }
+            run_src = in[i].data;
+            run_dst = job->plan.frames[i].bits_off;
+            run_len = in[i].len;
+        }
+        prev_end = in[i].data + in[i].len;
+    }
+    if (run_src) {
+        Status st = cuda_status(
+            cudaMemcpyAsync(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len, cudaMemcpyHostToDevice, s),
+            "bitstream upload");
+        if (st) return fail(st);
+    }
+    return PRORES_OK;
+}
+
+int prores_decode_job_launch(prores_decode_job *job, void *stream, int use_graph) {
+    Context &c = job->ctx->impl;
+    cudaSetDevice(c.device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
+    if (use_graph) {
+        if (!job->graph) {
+            cudaGraph_t g;
+            cudaStream_t cap = job->ws->stream;
+            Status st = cuda_status(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "capture");
+            if (!st) {
+                st = enqueue_decode(c, *job->ws, job->plan, cap, nullptr);
+                cudaError_t e = cudaStreamEndCapture(cap, &g);
+                if (!st) st = cuda_status(e, "capture");
+            }
+            if (!st) {
+                st = cuda_status(cudaGraphInstantiate(&job->graph, g, 0), "graph instantiate");
+                cudaGraphDestroy(g);
+            }
+            if (st) return fail(st);
+        }
+        return fail_or_ok(cuda_status(cudaGraphLaunch(job->graph, s), "graph launch"));
+    }
+    for (auto e : job->kt.events) cudaEventDestroy(e);
+    job->kt.events.clear();
+    job->kt.names.clear();
+    Status st = enqueue_decode(c, *job->ws, job->plan, s, &job->kt);
+    if (st) return fail(st);
+    return PRORES_OK;
+}
+
+int prores_decode_job_fetch(prores_decode_job *job, void *stream, prores_frame *out, int *status) {
+    cudaSetDevice(job->ctx->impl.device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
+    Status first;
+    Status st = fetch_decode(*job->ws, job->plan, s, out, status, &first);
+    if (st) return fail(st);
+    if (first) set_last_error(first);
+    return PRORES_OK;
+}
+
+int prores_decode_job_planes(prores_decode_job *job, int i, uint16_t **data, uint16_t **alpha) {
+    if (i < 0 || (size_t)i >= job->plan.frames.size()) return fail(make_status(PRORES_CONFIG, "no such frame"));
+    const DecodeFrame &f = job->plan.frames[i];
+    *data = job->ws->planes.as<uint16_t>() + f.plane_off;
+    *alpha = f.alpha_samples ? job->ws->alpha.as<uint16_t>() + f.alpha_off : nullptr;
+    return PRORES_OK;
+}
+
+int prores_job_kernel_times(const void *job, int is_encode, const char **names, float *ms, int cap) {
+    const KernelTimes &kt = is_encode ? static_cast<const prores_encode_job *>(job)->kt
+                                      : static_cast<const prores_decode_job *>(job)->kt;
+    if (!kt.enabled || kt.events.size() < 2) return 0;
+    if (cudaEventSynchronize(kt.events.back()) != cudaSuccess) return fail(make_status(PRORES_DEVICE, "event"));
+    int n = 0;
+    for (size_t i = 1; i < kt.events.size() && n < cap; i++, n++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, kt.events[i - 1], kt.events[i]);
+        names[n] = kt.names[i];
+        ms[n] = t;
+    }
+    return n;
+}
+
+void prores_decode_job_destroy(prores_decode_job *job) {
+    if (!job) return;
+    cudaSetDevice(job->ctx->impl.device);
+    if (job->graph) cudaGraphExecDestroy(job->graph);
+    for (auto e : job->kt.events) cudaEventDestroy(e);
+    if (job->ws) {
+        cudaStreamSynchronize(job->ws->stream);
+        job->ctx->impl.release(std::move(job->ws));
+    }
+    delete job;
+}
+
+}  // extern "C"

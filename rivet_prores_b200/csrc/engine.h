@@ -1,0 +1,145 @@
+// engine.h -- host side of the library: contexts, device workspaces, batch
+// plans and CUDA-graph capture around the decode and encode kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/prores_b200.h"
+#include "device_types.h"
+#include "host_headers.h"
+
+namespace prores {
+
+// A device allocation that only grows.
+struct DeviceBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes);
+    template <class T>
+    T *as() const {
+        return static_cast<T *>(p);
+    }
+    ~DeviceBuf();
+};
+
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t bytes);
+    ~PinnedBuf();
+};
+
+// Per-call device state: a stream and the buffers a batch needs.
+struct Workspace {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, planes, alpha, weights, counter;
+    // encode
+    DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
+        enc_alpha_bytes, enc_frame_out;
+    PinnedBuf host_stage;
+    bool coef_clean = true;  // the decode scratch is all zero
+    ~Workspace();
+};
+
+struct KernelTimes {
+    bool enabled = false;
+    std::vector<cudaEvent_t> events;
+    std::vector<const char *> names;
+    std::vector<float> ms;
+};
+
+struct Context {
+    int device = 0;
+    int sm_count = 0;
+    int entropy_grid = 0;
+    DeviceTables tables{};
+    std::mutex m;
+    std::vector<std::unique_ptr<Workspace>> free_ws;
+    std::unique_ptr<Workspace> acquire();
+    void release(std::unique_ptr<Workspace> ws);
+    ~Context();
+};
+
+Status cuda_status(cudaError_t e, const char *what);
+
+// ---- decode
+
+struct DecodeFrame {
+    Status err;  // a frame-header failure: nothing of the frame is decoded
+    FrameHeader hdr;
+    uint32_t depth = 0;
+    uint32_t first_pic = 0, n_pics = 0;  // pictures handed to the device
+    Status late;                         // a picture-level failure after those pictures
+    size_t bits_off = 0;
+    size_t plane_off = 0, samples = 0, alpha_off = 0, alpha_samples = 0;
+    int desc = -1;  // FrameDesc index
+};
+
+struct DecodePlan {
+    std::vector<DecodeFrame> frames;
+    std::vector<FrameDesc> fdesc;
+    std::vector<PicDesc> pdesc;
+    std::vector<uint8_t> weights;
+    size_t bits_total = 0, planes_total = 0, alpha_total = 0, coef_total = 0;
+    uint32_t n_slices = 0;
+    struct Copy {
+        const uint8_t *src;
+        size_t dst, len;
+    };
+    std::vector<Copy> copies;
+};
+
+Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan);
+Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s);
+Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s);
+DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan &plan);
+Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s, KernelTimes *kt);
+Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
+                    Status *first_err);
+
+// ---- encode
+
+struct EncodePlan;
+struct EncodePlanDeleter {
+    void operator()(EncodePlan *p) const;
+};
+using EncodePlanPtr = std::unique_ptr<EncodePlan, EncodePlanDeleter>;
+Status plan_encode(const prores_config *cfg, const prores_frame *in, int n, EncodePlanPtr &plan);
+Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores_frame *in, cudaStream_t s,
+                     bool descriptors);
+Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, KernelTimes *kt);
+Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s,
+                    std::vector<std::vector<uint8_t>> &out, int *status, Status *first_err);
+
+void set_last_error(const Status &s);
+// Per-frame messages of the last batch call on this thread.
+void set_batch_errors(const std::vector<Status> &errs);
+Status record_kernel(KernelTimes *kt, const char *name, cudaStream_t s);
+
+}  // namespace prores
+
+struct prores_ctx {
+    prores::Context impl;
+};
+
+struct prores_decode_job {
+    prores_ctx *ctx = nullptr;
+    std::unique_ptr<prores::Workspace> ws;
+    prores::DecodePlan plan;
+    cudaGraphExec_t graph = nullptr;
+    prores::KernelTimes kt;
+};
+
+struct prores_encode_job {
+    prores_ctx *ctx = nullptr;
+    std::unique_ptr<prores::Workspace> ws;
+    prores::EncodePlanPtr plan;
+    std::vector<std::vector<uint8_t>> packets;
+    prores::KernelTimes kt;
+};
