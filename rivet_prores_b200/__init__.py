@@ -516,3 +516,164 @@ class Encoder:
                 res.append(ctypes.string_at(outs[i].data, outs[i].len))
                 L.prores_buffer_free(outs[i].data)
         return res
+
+
+# ------------------------------------------------------------------ resident jobs
+
+def _as_u8(x) -> np.ndarray:
+    if isinstance(x, np.ndarray):
+        return x if x.dtype == np.uint8 else x.view(np.uint8)
+    return np.frombuffer(bytes(x), dtype=np.uint8)
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    """A cudaStream_t as an int: accepts None, an int, or any object with a
+    `cuda_stream` attribute (torch.cuda.Stream)."""
+    if stream is None:
+        return None
+    return int(getattr(stream, "cuda_stream", stream)) or None
+
+
+class DecodeJob:
+    """A batch of frames kept resident on the device: its bitstreams, slice
+    lists and planes stay allocated, so the batch is decoded again with no
+    host work (`launch`, optionally as one CUDA-graph launch), new bitstreams
+    of the same sizes can be copied in (`upload`) and the planes copied out
+    (`fetch`). The building block of batching and serving."""
+
+    def __init__(self, packets: Sequence, bit_depth: Optional[int] = None, device: int = 0):
+        self.device = device
+        self.n = len(packets)
+        self.depth = bit_depth or 0
+        self._ctx = context(device)
+        self._keep = [_as_u8(p) for p in packets]
+        bufs = self._bufs(self._keep)
+        h = ctypes.c_void_p()
+        _check(_abi.lib().prores_decode_job_create(self._ctx.handle, bufs, self.n, self.depth, ctypes.byref(h)))
+        self.handle = h
+        self.infos = []
+        for p in self._keep:
+            info = Frame_()
+            ok = _abi.lib().prores_probe(p.ctypes.data_as(ctypes.c_char_p), p.size, self.depth, ctypes.byref(info))
+            self.infos.append(info if ok == _abi.OK else None)
+
+    @staticmethod
+    def _bufs(arrays):
+        bufs = (Buf_ * max(len(arrays), 1))()
+        for i, a in enumerate(arrays):
+            bufs[i].data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+            bufs[i].len = a.size
+        return bufs
+
+    def upload(self, packets: Sequence, stream=None):
+        arrays = [_as_u8(p) for p in packets]
+        self._upload_keep = arrays
+        _check(_abi.lib().prores_decode_job_upload(self.handle, self._bufs(arrays), len(arrays), _stream_ptr(stream)))
+
+    def launch(self, stream=None, graph: bool = False):
+        _check(_abi.lib().prores_decode_job_launch(self.handle, _stream_ptr(stream), int(graph)))
+
+    def output_arrays(self, alloc=np.empty):
+        """Arrays for fetch(): (data, alpha) per frame, made by `alloc(n,
+        dtype)` (for example views of pinned memory)."""
+        out = []
+        for info in self.infos:
+            if info is None:
+                out.append((None, None))
+            else:
+                out.append((alloc(info.data_len, np.uint16),
+                            alloc(info.alpha_len, np.uint16) if info.alpha_len else None))
+        return out
+
+    def fetch(self, stream=None, arrays=None) -> List[Union[Frame, Error]]:
+        arrays = arrays if arrays is not None else self.output_arrays()
+        outs = (Frame_ * max(self.n, 1))()
+        status = (ctypes.c_int * max(self.n, 1))()
+        for i, (d, a) in enumerate(arrays):
+            if d is not None:
+                outs[i].data, outs[i].data_len = _ptr16(d), d.size
+            if a is not None:
+                outs[i].alpha, outs[i].alpha_len = _ptr16(a), a.size
+        _check(_abi.lib().prores_decode_job_fetch(self.handle, _stream_ptr(stream), outs, status))
+        res: List[Union[Frame, Error]] = []
+        for i in range(self.n):
+            if status[i] != _abi.OK:
+                res.append(_error(status[i], _abi.batch_error(i)))
+            else:
+                res.append(_frame_from_c(outs[i], arrays[i][0], arrays[i][1]))
+        return res
+
+    def kernel_times(self):
+        return _kernel_times(self.handle, 0)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _abi.lib().prores_decode_job_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class EncodeJob:
+    """The encode counterpart of DecodeJob: frames, coefficients, rate-control
+    tables and the output buffer stay resident; `fetch` returns the packets."""
+
+    def __init__(self, frames: Sequence[Frame], configs: Union[Config, Sequence[Config]], device: int = 0):
+        self.device = device
+        self.n = len(frames)
+        configs = [configs] * self.n if isinstance(configs, Config) else list(configs)
+        self._ctx = context(device)
+        self._keep = []
+        self._cfgs = (Config_ * max(self.n, 1))()
+        ins = (Frame_ * max(self.n, 1))()
+        for i in range(self.n):
+            self._cfgs[i] = configs[i]._c()
+            ins[i] = _frame_to_c(frames[i], self._keep)
+        h = ctypes.c_void_p()
+        _check(_abi.lib().prores_encode_job_create(self._ctx.handle, self._cfgs, ins, self.n, ctypes.byref(h)))
+        self.handle = h
+
+    def upload(self, frames: Sequence[Frame], stream=None):
+        keep = []
+        ins = (Frame_ * max(len(frames), 1))()
+        for i, f in enumerate(frames):
+            ins[i] = _frame_to_c(f, keep)
+        self._upload_keep = keep
+        _check(_abi.lib().prores_encode_job_upload(self.handle, ins, len(frames), _stream_ptr(stream)))
+
+    def launch(self, stream=None, graph: bool = False):
+        _check(_abi.lib().prores_encode_job_launch(self.handle, _stream_ptr(stream), int(graph)))
+
+    def fetch(self, stream=None, copy: bool = True) -> List[Union[bytes, memoryview, Error]]:
+        outs = (Buf_ * max(self.n, 1))()
+        status = (ctypes.c_int * max(self.n, 1))()
+        _check(_abi.lib().prores_encode_job_fetch(self.handle, _stream_ptr(stream), outs, status))
+        res: List[Union[bytes, memoryview, Error]] = []
+        for i in range(self.n):
+            if status[i] != _abi.OK:
+                res.append(_error(status[i], _abi.batch_error(i)))
+            elif copy:
+                res.append(ctypes.string_at(outs[i].data, outs[i].len))
+            else:
+                res.append(memoryview((ctypes.c_uint8 * outs[i].len).from_address(
+                    ctypes.addressof(outs[i].data.contents))) if outs[i].len else memoryview(b""))
+        return res
+
+    def kernel_times(self):
+        return _kernel_times(self.handle, 1)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _abi.lib().prores_encode_job_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+def _kernel_times(handle, is_encode: int):
+    """(name, ms) of each kernel of the job's last launch, when the job was
+    made with PRORES_PROFILE_KERNELS=1 in the environment."""
+    names = (ctypes.c_char_p * 64)()
+    ms = (ctypes.c_float * 64)()
+    n = _abi.lib().prores_job_kernel_times(handle, is_encode, names, ms, 64)
+    return [(names[i].decode(), float(ms[i])) for i in range(max(n, 0))]

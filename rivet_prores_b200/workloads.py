@@ -1,0 +1,88 @@
+"""Seeded synthetic pictures for the benchmark configurations.
+
+No public dataset is involved: each plane is generated at its own
+resolution as 512 + a sum of 8 random 2-D cosines (frequencies U(0, 0.05)
+cycles/px on each axis, amplitudes U(0, 150), phases U(0, 2 pi)) + 16
+axis-aligned rectangles set to a constant level U(64, 940) at positions and
+sizes uniform over the plane + Gaussian noise of sigma 12, clamped to 64-940
+(luma) or 64-960 (chroma) at 10-bit scale; 12- and 16-bit inputs are the
+10-bit picture shifted left by 2 and 6. The generator is numpy's PCG64 with
+seed = 1000 * config + frame index, and per-plane sub-seeds 0, 1, 2 (and 3
+for alpha: soft-edged ellipses over a 0 / max background plus sigma-200
+noise, clamped).
+"""
+
+from __future__ import annotations
+
+from typing import List, Optional
+
+import numpy as np
+
+from . import ChromaFormat, Config, Frame, Interlace, Profile
+
+
+def _plane(h: int, w: int, rng: np.random.Generator, hi: float) -> np.ndarray:
+    y = np.arange(h, dtype=np.float64)
+    x = np.arange(w, dtype=np.float64)
+    v = np.full((h, w), 512.0)
+    for _ in range(8):
+        fx, fy = rng.uniform(0.0, 0.05, 2)
+        amp = rng.uniform(0.0, 150.0)
+        phase = rng.uniform(0.0, 2 * np.pi)
+        # cos(a + b) = cos a cos b - sin a sin b: two outer products.
+        ax = 2 * np.pi * fx * x + phase
+        by = 2 * np.pi * fy * y
+        v += amp * (np.outer(np.cos(by), np.cos(ax)) - np.outer(np.sin(by), np.sin(ax)))
+    for _ in range(16):
+        x0, x1 = np.sort(rng.integers(0, w + 1, 2))
+        y0, y1 = np.sort(rng.integers(0, h + 1, 2))
+        v[y0:y1, x0:x1] = rng.uniform(64.0, 940.0)
+    v += rng.normal(0.0, 12.0, (h, w))
+    return np.clip(np.rint(v), 64.0, hi)
+
+
+def _alpha(h: int, w: int, rng: np.random.Generator) -> np.ndarray:
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    a = np.zeros((h, w))
+    for _ in range(4):
+        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
+        rx, ry = rng.uniform(0.1, 0.4) * w, rng.uniform(0.1, 0.4) * h
+        d = np.sqrt(((xx - cx) / rx) ** 2 + ((yy - cy) / ry) ** 2)
+        a = np.maximum(a, np.clip((1.0 - d) * 8.0, 0.0, 1.0))
+    a = a * 65535.0 + rng.normal(0.0, 200.0, (h, w))
+    return np.clip(np.rint(a), 0, 65535)
+
+
+def picture(width: int, height: int, chroma: ChromaFormat, bit_depth: int, seed: int,
+            alpha: bool = False, interlace: Interlace = Interlace.Progressive) -> Frame:
+    f = Frame.new(width, height, chroma, bit_depth)
+    f.interlace = interlace
+    for i in range(3):
+        p = f.planes[i]
+        rng = np.random.Generator(np.random.PCG64([seed, i]))
+        v = _plane(p.height, p.width, rng, 940.0 if i == 0 else 960.0)
+        v = v * float(1 << (bit_depth - 10)) if bit_depth >= 10 else np.rint(v / float(1 << (10 - bit_depth)))
+        f.data[p.offset:p.offset + p.len()] = v.astype(np.uint16).ravel()
+    if alpha:
+        rng = np.random.Generator(np.random.PCG64([seed, 3]))
+        a = _alpha(height, width, rng)
+        f.alpha = (a.astype(np.uint32) >> (16 - bit_depth)).astype(np.uint16).ravel()
+    return f
+
+
+def matrix(seed: int) -> bytes:
+    """A loaded quantisation matrix: 64 weights U(4, 63)."""
+    rng = np.random.Generator(np.random.PCG64([seed, 7]))
+    return bytes(int(v) for v in rng.integers(4, 64, 64))
+
+
+def uhd_422_hq(n: int, config: int = 1, unique: Optional[int] = None) -> List[Frame]:
+    """n 3840x2160 4:2:2 10-bit frames (the 422 HQ headline workload); with
+    `unique`, that many distinct pictures repeated."""
+    u = n if unique is None else max(1, min(unique, n))
+    base = [picture(3840, 2160, ChromaFormat.Yuv422, 10, 1000 * config + i) for i in range(u)]
+    return [base[i % u] for i in range(n)]
+
+
+def hq_config() -> Config:
+    return Config(Profile.Hq)
