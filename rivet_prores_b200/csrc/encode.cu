@@ -285,6 +285,7 @@ __device__ void alpha_write(const EncodeLaunch &e, const EncSliceDesc &sd, const
     const int lane = threadIdx.x & 31;
     const uint32_t n_runs = alpha_runs(e, sd, pd, fd, sc);
     const uint32_t bits = fd.alpha_bits;
+    const uint32_t max = bits == 8 ? 8u : 64u;
     uint64_t carry = 0;
     for (uint32_t base = 0; base < n_runs; base += 32) {
         const uint32_t j = base + lane;
@@ -301,7 +302,6 @@ __device__ void alpha_write(const EncodeLaunch &e, const EncSliceDesc &sd, const
             const int32_t prev = j ? (int32_t)sc.value[j - 1] : -1;
             const int32_t diff = (int32_t)sc.value[j] - prev;
             const uint32_t a = diff < 0 ? 0u - (uint32_t)diff : (uint32_t)diff;
-            const uint32_t mag = bits == 8 ? 3u : 6u, max = bits == 8 ? 8u : 64u;
             // Tables 13/14: `0`, |d| - 1, sign; or `1` and d mod 2^bits.
             if (a >= 1u && a <= max)
                 put_field(e.out, at, ((uint64_t)(a - 1u) << 1) | (uint64_t)(diff < 0), dlen);
@@ -317,11 +317,82 @@ __device__ void alpha_write(const EncodeLaunch &e, const EncSliceDesc &sd, const
 
 // ---------------------------------------------------------------- costing
 
-// Bits of one quantised component (src/encode.rs:383-409), one warp: lane l
-// takes scanned positions 32 k + l; each non-zero's run and its contexts
-// (the previous non-zero's run and level symbol) come from the lanes below
-// it or from what the last step carried.
-__device__ uint32_t component_bits(const float *f, uint32_t n_blocks, const float *inv) {
+// Codeword lengths of run and level symbols below 32 by context, kept in
+// shared memory by the kernels that count or write codes.
+struct LenTables {
+    uint8_t run[16][32];
+    uint8_t level[9][32];
+    __device__ void fill() {
+        for (uint32_t i = threadIdx.x; i < 16 * 32; i += blockDim.x) run[i >> 5][i & 31] = (uint8_t)cb_len(run_book(i >> 5), i & 31);
+        for (uint32_t i = threadIdx.x; i < 9 * 32; i += blockDim.x)
+            level[i >> 5][i & 31] = (uint8_t)cb_len(level_book(i >> 5), i & 31);
+    }
+    __device__ __forceinline__ uint32_t run_len(uint32_t ctx, uint32_t r) const {
+        const uint32_t c = ctx < 15u ? ctx : 15u;
+        return r < 32u ? run[c][r] : cb_len(run_book(c), r);
+    }
+    __device__ __forceinline__ uint32_t level_len(uint32_t ctx, uint32_t lvl) const {
+        const uint32_t c = ctx < 8u ? ctx : 8u;
+        return lvl < 32u ? level[c][lvl] : cb_len(level_book(c), lvl);
+    }
+};
+
+// The DC part of the bit count (src/encode.rs:383-395): EG5 of the first,
+// then Table 9 by |previous difference|, the sign flipped after a negative
+// one.
+__device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, float inv0) {
+    uint32_t bits = 0;
+    int32_t prev_dc = 0, prev_diff = 3;
+    for (uint32_t i = 0; i < n_blocks; i++) {
+        const int32_t q = quantise1(__ldg(f + i), inv0, 0.5f);
+        if (i == 0) {
+            bits += cb_len(kFirstDcBook, signed_to_symbol(q));
+        } else {
+            const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)prev_dc);
+            bits += cb_len(dc_book(prev_diff), signed_to_symbol(prev_diff < 0 ? -diff : diff));
+            prev_diff = diff;
+        }
+        prev_dc = q;
+    }
+    return bits;
+}
+
+// Bits of one quantised component (src/encode.rs:398-409), one lane: the
+// crate's own walk over the scanned positions, four coefficients a load.
+__device__ uint32_t lane_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
+    const uint32_t total = 64u * n_blocks;
+    const uint32_t shift = 31u - __clz(n_blocks);
+    uint32_t bits = dc_bits(f, n_blocks, __ldg(inv));
+    uint32_t prev_run = 4, prev_level = 1, pos = n_blocks;
+    for (uint32_t p0 = n_blocks & ~3u; p0 < total; p0 += 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+        const uint32_t s0 = p0 >> shift;
+        const float inv_a = __ldg(inv + s0), inv_b = __ldg(inv + min(s0 + 1u, 63u));
+#pragma unroll
+        for (uint32_t j = 0; j < 4; j++) {
+            const uint32_t p = p0 + j;
+            if (p < n_blocks) continue;
+            const int32_t q = quantise1(vv[j], ((p >> shift) == s0) ? inv_a : inv_b, kAcRounding);
+            if (q != 0) {
+                const uint32_t run = p - pos;
+                const uint32_t level = (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u;
+                bits += t.run_len(prev_run, run) + t.level_len(prev_level, level) + 1u;
+                prev_run = run;
+                prev_level = level;
+                pos = p + 1;
+            }
+        }
+    }
+    return bits;
+}
+
+// The same count with a whole warp on one component, for when latency
+// matters more than throughput (few items, or one slice the share-out
+// needs): lane l takes scanned positions 32 k + l; a non-zero's run and its
+// contexts (the previous non-zero's run and level symbol) come from the
+// lanes below it or from what the last step carried.
+__device__ uint32_t warp_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
     const int lane = threadIdx.x & 31;
     const uint32_t total = 64u * n_blocks;
     const uint32_t shift = 31u - __clz(n_blocks);
@@ -331,11 +402,9 @@ __device__ uint32_t component_bits(const float *f, uint32_t n_blocks, const floa
     for (uint32_t base = 0; base < total; base += 32) {
         const uint32_t p = base + lane;
         const uint32_t sidx = p >> shift;
-        const int32_t q = quantise1(f[p], __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
+        const int32_t q = quantise1(__ldg(f + p), __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
         if (base == 0) {
-            // The DCs (n_blocks <= 32, all in this step): EG5 of the first,
-            // then Table 9 by |previous difference|, sign flipped after a
-            // negative one.
+            // The DCs (n_blocks <= 32, all in this step).
             const int32_t left = __shfl_up_sync(0xffffffffu, q, 1);
             const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)left);
             const int32_t prev_diff_raw = __shfl_up_sync(0xffffffffu, diff, 1);
@@ -344,8 +413,7 @@ __device__ uint32_t component_bits(const float *f, uint32_t n_blocks, const floa
                     bits += cb_len(kFirstDcBook, signed_to_symbol(q));
                 } else {
                     const int32_t prev_diff = p == 1 ? 3 : prev_diff_raw;
-                    const int32_t n = prev_diff < 0 ? -diff : diff;
-                    bits += cb_len(dc_book(prev_diff), signed_to_symbol(n));
+                    bits += cb_len(dc_book(prev_diff), signed_to_symbol(prev_diff < 0 ? -diff : diff));
                 }
             }
         }
@@ -359,11 +427,7 @@ __device__ uint32_t component_bits(const float *f, uint32_t n_blocks, const floa
         const uint32_t level = nz ? (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u : 0u;
         const uint32_t src_run = __shfl_sync(0xffffffffu, run, src);
         const uint32_t src_level = __shfl_sync(0xffffffffu, level, src);
-        if (nz) {
-            const uint32_t ctx_run = below ? src_run : carry_run;
-            const uint32_t ctx_level = below ? src_level : carry_level;
-            bits += cb_len(run_book(ctx_run), run) + cb_len(level_book(ctx_level), level) + 1u;
-        }
+        if (nz) bits += t.run_len(below ? src_run : carry_run, run) + t.level_len(below ? src_level : carry_level, level) + 1u;
         const int top = 31 - __clz(mask);
         carry_pos = (int32_t)(base + top);
         carry_run = __shfl_sync(0xffffffffu, run, top);
@@ -386,19 +450,52 @@ __device__ __forceinline__ void comp_layout(const EncFrameDesc &fd, uint32_t mbs
     offset = comp == 0 ? 0u : 64u * mbs * (4u + (comp - 1u) * cpm);
 }
 
-// Bytes of one slice component at quantiser qi.
+// Bytes of one slice component at quantiser qi (one lane).
 __device__ __forceinline__ uint32_t component_bytes(const EncodeLaunch &e, const EncSliceDesc &sd, const EncPicDesc &pd,
-                                                    const EncFrameDesc &fd, uint32_t comp, uint32_t qi) {
+                                                    const EncFrameDesc &fd, uint32_t comp, uint32_t qi,
+                                                    const LenTables &t) {
     uint32_t nb, off;
     comp_layout(fd, sd.mbs, comp, nb, off);
-    const uint32_t bits = component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp));
+    const uint32_t bits = lane_component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp), t);
     return (bits + 7u) / 8u;
 }
 
-constexpr int kCostWarps = 8;
+// Bytes of one slice component at quantiser qi, the whole warp.
+__device__ __forceinline__ uint32_t warp_component_bytes(const EncodeLaunch &e, const EncSliceDesc &sd,
+                                                         const EncPicDesc &pd, const EncFrameDesc &fd, uint32_t comp,
+                                                         uint32_t qi, const LenTables &t) {
+    uint32_t nb, off;
+    comp_layout(fd, sd.mbs, comp, nb, off);
+    const uint32_t bits = warp_component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp), t);
+    return (bits + 7u) / 8u;
+}
 
-__global__ void __launch_bounds__(32 * kCostWarps) k_cost(EncodeLaunch e, int step) {
-    const uint32_t item = blockIdx.x * kCostWarps + (threadIdx.x >> 5);
+constexpr int kCostThreads = 256;
+
+// Work items are (component, slice), component-major: a warp's lanes take
+// the same component of 32 neighbouring slices, which cost about the same.
+__global__ void __launch_bounds__(kCostThreads) k_cost(EncodeLaunch e, int step) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
+    const uint32_t item = blockIdx.x * kCostThreads + threadIdx.x;
+    if (item >= 3u * e.n_slices) return;
+    const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
+    const EncSliceDesc sd = e.slices[s];
+    const int32_t qi = e.state[sd.pic].probe_qi;
+    if (qi == 0) return;
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    e.probe_comp[((uint64_t)step * e.n_slices + s) * 3u + comp] = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+}
+
+// k_cost with a warp per item, for batches too small to fill the GPU with
+// one lane per item.
+__global__ void __launch_bounds__(kCostThreads) k_cost_warp(EncodeLaunch e, int step) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
+    const uint32_t item = blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5);
     if (item >= 3u * e.n_slices) return;
     const uint32_t s = item / 3u, comp = item - 3u * s;
     const EncSliceDesc sd = e.slices[s];
@@ -406,25 +503,8 @@ __global__ void __launch_bounds__(32 * kCostWarps) k_cost(EncodeLaunch e, int st
     if (qi == 0) return;
     const EncPicDesc &pd = e.pics[sd.pic];
     const EncFrameDesc &fd = e.frames[pd.frame];
-    const uint32_t bytes = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi);
+    const uint32_t bytes = warp_component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
     if ((threadIdx.x & 31) == 0) e.probe_comp[((uint64_t)step * e.n_slices + s) * 3u + comp] = bytes;
-}
-
-__global__ void __launch_bounds__(32 * kCostWarps) k_cost_window(EncodeLaunch e) {
-    const uint32_t item = blockIdx.x * kCostWarps + (threadIdx.x >> 5);
-    if (item >= 3u * kWindow * e.n_slices) return;
-    const uint32_t j = item / (3u * e.n_slices);
-    const uint32_t r = item - j * 3u * e.n_slices;
-    const uint32_t s = r / 3u, comp = r - 3u * s;
-    const EncSliceDesc sd = e.slices[s];
-    const EncPicState st = e.state[sd.pic];
-    if (!(st.fits_at_all && st.uniform > 1)) return;
-    const int32_t qi = st.uniform - 1 - (int32_t)j;
-    if (qi < 1) return;
-    const EncPicDesc &pd = e.pics[sd.pic];
-    const EncFrameDesc &fd = e.frames[pd.frame];
-    const uint32_t bytes = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi);
-    if ((threadIdx.x & 31) == 0) e.win_comp[((uint64_t)j * e.n_slices + s) * 3u + comp] = bytes;
 }
 
 // A slice's size from its component bytes, and whether every 16-bit size
@@ -433,6 +513,70 @@ __device__ __forceinline__ uint64_t slice_total(uint32_t hdr, const uint32_t c[3
     const uint64_t t = (uint64_t)hdr + c[0] + c[1] + c[2] + alpha;
     fits = t <= 65535u && c[0] <= 65535u && c[1] <= 65535u && c[2] <= 65535u;
     return t;
+}
+
+// Macroblocks from slice (mb_x, mb_y) to the end of the picture: the
+// share-out's remaining_mbs (src/encode.rs:737-741, :771).
+__device__ __forceinline__ uint64_t mbs_from(const EncPicDesc &pd, const EncSliceDesc &sd) {
+    return (uint64_t)pd.width_in_mb * pd.height_in_mb - ((uint64_t)sd.mb_y * pd.width_in_mb + sd.mb_x);
+}
+
+// Component sizes at window level j (quantiser uniform - 1 - j) of slice s:
+// from the failed probe at uniform - 1 when there is one, else the window.
+__device__ __forceinline__ const uint32_t *level_comp(const EncodeLaunch &e, const EncPicState &st, uint32_t j,
+                                                      uint32_t s) {
+    if (j == 0 && st.lo_probe >= 0) return e.probe_comp + ((uint64_t)st.lo_probe * e.n_slices + s) * 3u;
+    return e.win_comp + ((uint64_t)j * e.n_slices + s) * 3u;
+}
+
+// Window level j: the first for every slice; the next ones for the slices
+// whose size at the level before fits and is within the most their share
+// can come to (the crate's prefetch rule, src/encode.rs:741-767).
+template <bool kWarp>
+__global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, int level) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
+    const uint32_t item = kWarp ? blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5)
+                                : blockIdx.x * kCostThreads + threadIdx.x;
+    if (item >= 3u * e.n_slices) return;
+    const uint32_t comp = kWarp ? item % 3u : item / e.n_slices;
+    const uint32_t s = kWarp ? item / 3u : item - comp * e.n_slices;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicState st = e.state[sd.pic];
+    if (!(st.fits_at_all && st.uniform > 1)) return;
+    const int32_t qi = st.uniform - 1 - level;
+    if (qi < 1) return;
+    if (level == 0 && st.lo_probe >= 0) return;  // probed already
+    const EncPicDesc &pd = e.pics[sd.pic];
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    uint32_t *out = e.win_comp + ((uint64_t)level * e.n_slices + s) * 3u;
+    if (level > 0) {
+        const uint32_t *prev = level_comp(e, st, (uint32_t)level - 1u, s);
+        bool wanted = prev[0] != kNotCosted;
+        if (wanted) {
+            const uint32_t alpha = e.alpha_bytes[s];
+            const uint32_t pc[3] = {prev[0], prev[1], prev[2]};
+            bool fits, f2;
+            const uint64_t n = slice_total(pd.header_bytes, pc, alpha, fits);
+            const uint32_t *u = e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u;
+            const uint32_t uc[3] = {u[0], u[1], u[2]};
+            const uint64_t used = slice_total(pd.header_bytes, uc, alpha, f2);
+            const uint64_t slack = st.budget - st.hi_total;
+            const uint64_t most = used + slack * sd.mbs / mbs_from(pd, sd);
+            wanted = fits && n <= most;
+        }
+        if (!wanted) {
+            if (comp == 0 && (!kWarp || (threadIdx.x & 31) == 0)) out[0] = kNotCosted;
+            return;
+        }
+    }
+    if (kWarp) {
+        const uint32_t bytes = warp_component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+        if ((threadIdx.x & 31) == 0) out[comp] = bytes;
+    } else {
+        out[comp] = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+    }
 }
 
 constexpr int kRcThreads = 256;
@@ -466,6 +610,7 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_init(EncodeLaunch e) {
         st.hi = 224;
         st.probe_qi = 224;
         st.hi_probe = 0;
+        st.lo_probe = -1;
         st.fits_at_all = 0;
         st.uniform = 224;
         e.state[blockIdx.x] = st;
@@ -500,6 +645,7 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
             // used throughout (src/encode.rs:701-713).
             st.fits_at_all = ok;
             st.hi_probe = 0;
+            st.hi_total = total;
             if (!ok) {
                 st.probe_qi = 0;
                 st.uniform = 224;
@@ -507,8 +653,10 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
         } else if (ok) {
             st.hi = st.probe_qi;
             st.hi_probe = step;
+            st.hi_total = total;
         } else {
             st.lo = st.probe_qi + 1;
+            st.lo_probe = step;
         }
         if (st.fits_at_all) {
             if (st.lo < st.hi) {
@@ -522,12 +670,20 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
     }
 }
 
-// The share-out (src/encode.rs:769-793): one warp per picture walks its
-// slices in order; every lane runs the same recurrence so that the warp can
-// cost a deeper quantiser together when one is needed.
+// The share-out (src/encode.rs:769-793), one warp per picture. With
+// D = remaining_budget - remaining_base, slice i steps from the uniform
+// quantiser to the next finer one while that size n fits and
+// n <= base + floor(D mbs / remaining_mbs), i.e. while n <= base or
+// D >= ceil((n - base) remaining_mbs / mbs); D then falls by what the slice
+// took over its base. Each lane works out its slice's thresholds; the walk
+// itself only compares D with them, 32 slices at a time by ballot, and
+// costs a deeper quantiser with the warp when a slice gets that far.
 constexpr int kShareWarps = 4;
 
 __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
     const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
     if (p >= e.n_pics) return;
     const int lane = threadIdx.x & 31;
@@ -536,94 +692,130 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     const EncFrameDesc &fd = e.frames[pd.frame];
     const uint32_t *used_c = e.probe_comp + (uint64_t)st.hi_probe * e.n_slices * 3u;
     const uint32_t hb = pd.header_bytes;
-    if (!(st.uniform > 1 && st.fits_at_all)) {
-        for (uint32_t k = lane; k < pd.n_slices; k += 32) {
-            const uint32_t s = pd.slice_base + k;
-            e.final_qi[s] = (uint32_t)st.uniform;
-            for (int c = 0; c < 3; c++) e.final_comp[3ull * s + c] = used_c[3ull * s + c];
-        }
-        return;
-    }
-    uint64_t used_sum = 0, mbs_sum = 0;
-    for (uint32_t k = lane; k < pd.n_slices; k += 32) {
-        const uint32_t s = pd.slice_base + k;
-        const uint32_t cc[3] = {used_c[3ull * s], used_c[3ull * s + 1], used_c[3ull * s + 2]};
-        bool f;
-        used_sum += slice_total(hb, cc, e.alpha_bytes[s], f);
-        mbs_sum += e.slices[s].mbs;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        used_sum += __shfl_xor_sync(0xffffffffu, used_sum, o);
-        mbs_sum += __shfl_xor_sync(0xffffffffu, mbs_sum, o);
-    }
-    uint64_t rem_budget = st.budget, rem_base = used_sum, rem_mbs = mbs_sum;
+    const bool refine = st.uniform > 1 && st.fits_at_all;
+    uint64_t D = refine ? st.budget - st.hi_total : 0;
     for (uint32_t k0 = 0; k0 < pd.n_slices; k0 += 32) {
-        // Each lane fetches one of the next 32 slices' sizes; the walk then
-        // reads them by shuffles.
         const uint32_t k = k0 + lane;
-        uint32_t my_mbs = 0, my_alpha = 0, u0 = 0, u1 = 0, u2 = 0, w0 = 0, w1 = 0, w2 = 0;
-        if (k < pd.n_slices) {
-            const uint32_t s = pd.slice_base + k;
-            my_mbs = e.slices[s].mbs;
-            my_alpha = e.alpha_bytes[s];
-            u0 = used_c[3ull * s];
-            u1 = used_c[3ull * s + 1];
-            u2 = used_c[3ull * s + 2];
-            const uint32_t *w = e.win_comp + 3ull * s;
-            w0 = w[0];
-            w1 = w[1];
-            w2 = w[2];
-        }
-        const uint32_t count = min(32u, pd.n_slices - k0);
-        for (uint32_t i = 0; i < count; i++) {
-            const uint32_t s = pd.slice_base + k0 + i;
-            const uint32_t mbs = __shfl_sync(0xffffffffu, my_mbs, i);
-            const uint32_t alpha = __shfl_sync(0xffffffffu, my_alpha, i);
-            uint32_t cur[3] = {__shfl_sync(0xffffffffu, u0, i), __shfl_sync(0xffffffffu, u1, i),
-                               __shfl_sync(0xffffffffu, u2, i)};
-            const uint32_t first[3] = {__shfl_sync(0xffffffffu, w0, i), __shfl_sync(0xffffffffu, w1, i),
-                                       __shfl_sync(0xffffffffu, w2, i)};
+        const bool live = k < pd.n_slices;
+        const uint32_t s = pd.slice_base + (live ? k : 0u);
+        uint32_t base_c[3] = {0, 0, 0}, alpha = 0, mbs = 1, shift = 0;
+        uint64_t base = 0, rem = 1;
+        uint64_t thr[kWindow];
+        uint64_t size[kWindow];
+        bool ok[kWindow];
+        if (live) {
+            const EncSliceDesc sd = e.slices[s];
+            base_c[0] = used_c[3ull * s];
+            base_c[1] = used_c[3ull * s + 1];
+            base_c[2] = used_c[3ull * s + 2];
+            alpha = e.alpha_bytes[s];
+            mbs = sd.mbs;
+            shift = 31u - __clz(mbs);
+            rem = mbs_from(pd, sd);
             bool f;
-            const uint64_t base = slice_total(hb, cur, alpha, f);
-            const uint64_t slack = rem_budget - rem_base;
-            const uint64_t allowed = base + slack * mbs / rem_mbs;
-            uint64_t used = base;
-            int32_t qi = st.uniform;
-            while (qi > 1) {
-                const uint32_t stepd = (uint32_t)(st.uniform - qi);
-                uint32_t c3[3];
-                if (stepd == 0) {
-                    c3[0] = first[0];
-                    c3[1] = first[1];
-                    c3[2] = first[2];
-                } else if (stepd < (uint32_t)kWindow) {
-                    const uint32_t *w = e.win_comp + ((uint64_t)stepd * e.n_slices + s) * 3u;
-                    c3[0] = w[0];
-                    c3[1] = w[1];
-                    c3[2] = w[2];
-                } else {
-                    const EncSliceDesc sd = e.slices[s];
-                    for (uint32_t c = 0; c < 3; c++) c3[c] = component_bytes(e, sd, pd, fd, c, (uint32_t)(qi - 1));
+            base = slice_total(hb, base_c, alpha, f);
+        }
+#pragma unroll
+        for (int j = 0; j < kWindow; j++) {
+            ok[j] = false;
+            size[j] = 0;
+            thr[j] = ~0ull;
+            if (!(live && refine) || st.uniform - j <= 1) continue;
+            const uint32_t *c = level_comp(e, st, (uint32_t)j, s);
+            if (c[0] == kNotCosted) continue;  // unknown: costed below if reached
+            const uint32_t cc[3] = {c[0], c[1], c[2]};
+            bool fits;
+            size[j] = slice_total(hb, cc, alpha, fits);
+            ok[j] = true;
+            // Known, but never taken when it does not fit.
+            thr[j] = !fits ? ~0ull : (size[j] <= base ? 0ull : (((size[j] - base) * rem + mbs - 1) >> shift));
+        }
+        uint32_t my_qi = (uint32_t)st.uniform, my_steps = 0;
+        uint32_t deep_c[3] = {0, 0, 0};
+        if (refine) {
+            uint32_t done = 0;  // lanes below this have been walked
+            while (done < 32u && k0 + done < pd.n_slices) {
+                // The first slice from `done` on that steps at all, at this D
+                // (its first level unknown counts as "might").
+                const bool steps = live && lane >= (int)done && (!ok[0] ? st.uniform > 1 : D >= thr[0]);
+                const uint32_t mask = __ballot_sync(0xffffffffu, steps);
+                if (!mask) break;
+                const uint32_t f = __ffs(mask) - 1;
+                // Walk slice f with the whole warp: its allowed size is fixed
+                // while it steps, so every finer quantiser is a separate test.
+                const uint64_t fbase = __shfl_sync(0xffffffffu, base, f);
+                const uint32_t fmbs = __shfl_sync(0xffffffffu, mbs, f);
+                const uint64_t frem = __shfl_sync(0xffffffffu, rem, f);
+                const uint32_t falpha = __shfl_sync(0xffffffffu, alpha, f);
+                const uint64_t allowed = fbase + D * fmbs / frem;
+                int32_t qi = st.uniform;
+                uint64_t used = fbase;
+                uint32_t stepsf = 0;
+                bool stop = false, deep = false;
+                uint32_t dc[3] = {0, 0, 0};
+#pragma unroll
+                for (int jj = 0; jj < kWindow; jj++) {
+                    if (stop || qi <= 1) break;
+                    const bool known = __shfl_sync(0xffffffffu, ok[jj], f);
+                    if (!known) break;
+                    const uint64_t n = __shfl_sync(0xffffffffu, size[jj], f);
+                    const bool fits = __shfl_sync(0xffffffffu, thr[jj], f) != ~0ull;
+                    if (!(fits && n <= allowed)) {
+                        stop = true;
+                        break;
+                    }
+                    qi -= 1;
+                    used = n;
+                    stepsf++;
                 }
-                bool fits;
-                const uint64_t n = slice_total(hb, c3, alpha, fits);
-                if (!(fits && n <= allowed)) break;
-                qi -= 1;
-                used = n;
-                cur[0] = c3[0];
-                cur[1] = c3[1];
-                cur[2] = c3[2];
+                // Deeper: the warp costs quantiser qi - 1, a component at a
+                // time, and the slice steps while it fits its allowance.
+                const EncSliceDesc fsd = e.slices[pd.slice_base + k0 + f];
+                while (!stop && qi > 1) {
+                    uint32_t c3[3];
+                    for (uint32_t c = 0; c < 3; c++) c3[c] = warp_component_bytes(e, fsd, pd, fd, c, (uint32_t)(qi - 1), t);
+                    bool fits;
+                    const uint64_t n = slice_total(hb, c3, falpha, fits);
+                    if (!(fits && n <= allowed)) break;
+                    qi -= 1;
+                    used = n;
+                    stepsf++;
+                    dc[0] = c3[0];
+                    dc[1] = c3[1];
+                    dc[2] = c3[2];
+                    deep = true;
+                }
+                if (lane == (int)f) {
+                    my_qi = (uint32_t)qi;
+                    my_steps = stepsf;
+                    if (deep) {
+                        deep_c[0] = dc[0];
+                        deep_c[1] = dc[1];
+                        deep_c[2] = dc[2];
+                        my_steps |= 0x80000000u;  // sizes in deep_c
+                    }
+                }
+                D = D + fbase - used;
+                done = f + 1;
             }
-            if (lane == 0) {
-                e.final_qi[s] = (uint32_t)qi;
-                e.final_comp[3ull * s] = cur[0];
-                e.final_comp[3ull * s + 1] = cur[1];
-                e.final_comp[3ull * s + 2] = cur[2];
+        }
+        if (live) {
+            e.final_qi[s] = my_qi;
+            uint32_t c3[3] = {base_c[0], base_c[1], base_c[2]};
+            const uint32_t nsteps = my_steps & 0x7FFFFFFFu;
+            if (my_steps & 0x80000000u) {
+                c3[0] = deep_c[0];
+                c3[1] = deep_c[1];
+                c3[2] = deep_c[2];
+            } else if (nsteps > 0) {
+                const uint32_t *c = level_comp(e, st, nsteps - 1u, s);
+                c3[0] = c[0];
+                c3[1] = c[1];
+                c3[2] = c[2];
             }
-            rem_budget -= used;
-            rem_base -= base;
-            rem_mbs -= mbs;
+            e.final_comp[3ull * s] = c3[0];
+            e.final_comp[3ull * s + 1] = c3[1];
+            e.final_comp[3ull * s + 2] = c3[2];
         }
     }
 }
@@ -706,125 +898,183 @@ __global__ void k_frame(EncodeLaunch e) {
 
 // ---------------------------------------------------------------- packing
 
-// Writes one quantised component's codes (src/encode.rs:413-437) from bit
-// `bitpos`: each lane's codeword lengths, scanned across the warp, give its
-// place.
-__device__ void component_write(uint32_t *out, uint64_t bitpos, const float *f, uint32_t n_blocks, const float *inv) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t total = 64u * n_blocks;
-    const uint32_t shift = 31u - __clz(n_blocks);
-    uint64_t carry_bits = 0;
-    int32_t carry_pos = (int32_t)n_blocks - 1;
-    uint32_t carry_run = 4, carry_level = 1;
-    for (uint32_t base = 0; base < total; base += 32) {
-        const uint32_t p = base + lane;
-        const uint32_t sidx = p >> shift;
-        const int32_t q = quantise1(f[p], __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
-        uint32_t len = 0;
-        uint64_t cw0 = 0, cw1 = 0;
-        uint32_t l0 = 0, l1 = 0;
-        bool neg = false;
-        if (base == 0) {
-            const int32_t left = __shfl_up_sync(0xffffffffu, q, 1);
-            const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)left);
-            const int32_t prev_diff_raw = __shfl_up_sync(0xffffffffu, diff, 1);
-            if (p < n_blocks) {
-                Codebook cb;
-                uint32_t sym;
-                if (p == 0) {
-                    cb = kFirstDcBook;
-                    sym = signed_to_symbol(q);
-                } else {
-                    const int32_t prev_diff = p == 1 ? 3 : prev_diff_raw;
-                    cb = dc_book(prev_diff);
-                    sym = signed_to_symbol(prev_diff < 0 ? -diff : diff);
-                }
-                cw0 = cb_bits(cb, sym);
-                l0 = cb_len(cb, sym);
-                len = l0;
-            }
-        }
-        const bool nz = q != 0 && p >= n_blocks;
-        const uint32_t mask = __ballot_sync(0xffffffffu, nz);
-        const uint32_t below = mask & ((1u << lane) - 1u);
-        const int src = below ? 31 - __clz(below) : lane;
-        const int32_t prev_pos = below ? (int32_t)(base + src) : carry_pos;
-        const uint32_t run = nz ? (uint32_t)((int32_t)p - prev_pos - 1) : 0u;
-        const uint32_t level = nz ? (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u : 0u;
-        const uint32_t src_run = __shfl_sync(0xffffffffu, run, src);
-        const uint32_t src_level = __shfl_sync(0xffffffffu, level, src);
-        if (nz) {
-            const Codebook rb = run_book(below ? src_run : carry_run);
-            const Codebook lb = level_book(below ? src_level : carry_level);
-            cw0 = cb_bits(rb, run);
-            l0 = cb_len(rb, run);
-            cw1 = cb_bits(lb, level);
-            l1 = cb_len(lb, level);
-            neg = q < 0;
-            len = l0 + l1 + 1u;
-        }
-        uint64_t incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (len) {
-            const uint64_t at = bitpos + carry_bits + incl - len;
-            put_field(out, at, cw0, l0);
-            if (nz) {
-                put_field(out, at + l0, cw1, l1);
-                if (neg) put_field(out, at + l0 + l1, 1u, 1u);
-            }
-        }
-        carry_bits += __shfl_sync(0xffffffffu, incl, 31);
-        if (mask) {
-            const int top = 31 - __clz(mask);
-            carry_pos = (int32_t)(base + top);
-            carry_run = __shfl_sync(0xffffffffu, run, top);
-            carry_level = __shfl_sync(0xffffffffu, level, top);
+// An MSB-first writer into the big-endian output words from an absolute
+// bit position. Words wholly inside the writer's bytes are stored; the
+// partial words at either end, which a neighbour shares, are OR-ed.
+struct BitOut {
+    uint32_t *out;
+    uint64_t cur;  // absolute position of the first bit held
+    uint64_t acc;
+    uint32_t nacc;
+    __device__ __forceinline__ void init(uint32_t *o, uint64_t bitpos) {
+        out = o;
+        cur = bitpos;
+        acc = 0;
+        nacc = 0;
+    }
+    __device__ __forceinline__ void emit() {
+        for (;;) {
+            const uint32_t room = 32u - (uint32_t)(cur & 31u);
+            if (nacc < room) return;
+            const uint32_t chunk = (uint32_t)(acc >> (nacc - room)) & (room == 32u ? 0xFFFFFFFFu : ((1u << room) - 1u));
+            uint32_t *w = out + (cur >> 5);
+            if (room == 32u)
+                *w = bswap32(chunk);
+            else
+                atomicOr(w, bswap32(chunk));
+            nacc -= room;
+            cur += room;
         }
     }
+    // A field of n <= 32 bits holding v.
+    __device__ __forceinline__ void put(uint64_t v, uint32_t n) {
+        if (n == 0) return;
+        acc = (acc << n) | v;
+        nacc += n;
+        emit();
+    }
+    // A field of any width holding v (its leading zeros included).
+    __device__ __forceinline__ void put_long(uint64_t v, uint32_t n) {
+        if (n > 64) {
+            put(0, n - 64);
+            n = 64;
+        }
+        if (n > 32) {
+            put(v >> 32, n - 32);
+            v &= 0xFFFFFFFFull;
+            n = 32;
+        }
+        put(v, n);
+    }
+    // Zero bits to the next byte boundary, then the last partial word.
+    __device__ __forceinline__ void finish() {
+        const uint32_t pad = (uint32_t)((8u - ((cur + nacc) & 7u)) & 7u);
+        put(0, pad);
+        if (nacc) {
+            const uint32_t room = 32u - (uint32_t)(cur & 31u);
+            const uint32_t chunk = (uint32_t)(acc & ((1ull << nacc) - 1)) << (room - nacc);
+            atomicOr(out + (cur >> 5), bswap32(chunk));
+            cur += nacc;
+            nacc = 0;
+        }
+    }
+};
+
+// One quantised component's codes (src/encode.rs:413-437), one lane.
+__device__ void lane_component_write(BitOut &w, const float *f, uint32_t n_blocks, const float *inv,
+                                     const LenTables &t) {
+    const uint32_t total = 64u * n_blocks;
+    const uint32_t shift = 31u - __clz(n_blocks);
+    const float inv0 = __ldg(inv);
+    int32_t prev_dc = 0, prev_diff = 3;
+    for (uint32_t i = 0; i < n_blocks; i++) {
+        const int32_t q = quantise1(__ldg(f + i), inv0, 0.5f);
+        Codebook cb;
+        uint32_t sym;
+        if (i == 0) {
+            cb = kFirstDcBook;
+            sym = signed_to_symbol(q);
+        } else {
+            const int32_t diff = (int32_t)((uint32_t)q - (uint32_t)prev_dc);
+            cb = dc_book(prev_diff);
+            sym = signed_to_symbol(prev_diff < 0 ? -diff : diff);
+            prev_diff = diff;
+        }
+        w.put_long(cb_bits(cb, sym), cb_len(cb, sym));
+        prev_dc = q;
+    }
+    uint32_t prev_run = 4, prev_level = 1, pos = n_blocks;
+    for (uint32_t p0 = n_blocks & ~3u; p0 < total; p0 += 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+        const float vv[4] = {v.x, v.y, v.z, v.w};
+        const uint32_t s0 = p0 >> shift;
+        const float inv_a = __ldg(inv + s0), inv_b = __ldg(inv + min(s0 + 1u, 63u));
+#pragma unroll
+        for (uint32_t j = 0; j < 4; j++) {
+            const uint32_t p = p0 + j;
+            if (p < n_blocks) continue;
+            const int32_t q = quantise1(vv[j], ((p >> shift) == s0) ? inv_a : inv_b, kAcRounding);
+            if (q != 0) {
+                const uint32_t run = p - pos;
+                const uint32_t level = (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u;
+                const Codebook rb = run_book(prev_run), lb = level_book(prev_level);
+                const uint32_t rl = t.run_len(prev_run, run), ll = t.level_len(prev_level, level);
+                if (rl + ll + 1u <= 32u) {
+                    w.put((((cb_bits(rb, run) << ll) | cb_bits(lb, level)) << 1) | (uint64_t)(q < 0), rl + ll + 1u);
+                } else {
+                    w.put_long(cb_bits(rb, run), rl);
+                    w.put_long(cb_bits(lb, level), ll);
+                    w.put((uint64_t)(q < 0), 1);
+                }
+                prev_run = run;
+                prev_level = level;
+                pos = p + 1;
+            }
+        }
+    }
+    w.finish();
 }
 
-__global__ void __launch_bounds__(128) k_pack(EncodeLaunch e) {
-    __shared__ AlphaScratch scratch;
-    const uint32_t s = blockIdx.x;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Each slice component's codes, one lane per (component, slice).
+__global__ void __launch_bounds__(kCostThreads) k_pack(EncodeLaunch e) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
+    const uint32_t item = blockIdx.x * kCostThreads + threadIdx.x;
+    if (item >= 3u * e.n_slices) return;
+    const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    if (e.frame_status[pd.frame]) return;
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const EncPicState &st = e.state[sd.pic];
+    uint64_t at = 8ull * (fd.out_base + st.pic_off + e.slice_off[s] + pd.header_bytes);
+    for (uint32_t c = 0; c < comp; c++) at += 8ull * e.final_comp[3ull * s + c];
+    uint32_t nb, off;
+    comp_layout(fd, sd.mbs, comp, nb, off);
+    BitOut w;
+    w.init(e.out, at);
+    lane_component_write(w, e.coef + sd.coef + off, nb, quant_table(e, pd, e.final_qi[s], comp), t);
+}
+
+// Slice headers and table entries, one thread per slice; alpha codes, one
+// warp per slice.
+__global__ void k_pack_headers(EncodeLaunch e) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= e.n_slices) return;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    if (e.frame_status[pd.frame]) return;
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const EncPicState &st = e.state[sd.pic];
+    const uint32_t comp[3] = {e.final_comp[3ull * s], e.final_comp[3ull * s + 1], e.final_comp[3ull * s + 2]};
+    const uint32_t hb = pd.header_bytes;
+    const uint64_t slice_bit = 8ull * (fd.out_base + st.pic_off + e.slice_off[s]);
+    bool f;
+    const uint64_t total = slice_total(hb, comp, e.alpha_bytes[s], f);
+    // slice_header_size << 3, quantization_index, the component sizes (the
+    // Cr size only with alpha); the slice table's entry.
+    put_field(e.out, slice_bit, hb << 3, 8);
+    put_field(e.out, slice_bit + 8, e.final_qi[s], 8);
+    put_field(e.out, slice_bit + 16, comp[0] & 0xFFFFu, 16);
+    put_field(e.out, slice_bit + 32, comp[1] & 0xFFFFu, 16);
+    if (hb == 8) put_field(e.out, slice_bit + 48, comp[2] & 0xFFFFu, 16);
+    const uint64_t table_bit = 8ull * (fd.out_base + st.pic_off + 8u + 2ull * (s - pd.slice_base));
+    put_field(e.out, table_bit, (uint32_t)(total & 0xFFFFu), 16);
+}
+
+__global__ void __launch_bounds__(32 * kAlphaWarps) k_pack_alpha(EncodeLaunch e) {
+    __shared__ AlphaScratch scratch[kAlphaWarps];
+    const uint32_t s = blockIdx.x * kAlphaWarps + (threadIdx.x >> 5);
+    if (s >= e.n_slices) return;
     const EncSliceDesc sd = e.slices[s];
     const EncPicDesc &pd = e.pics[sd.pic];
     const EncFrameDesc &fd = e.frames[pd.frame];
-    if (e.frame_status[pd.frame]) return;
+    if (!fd.alpha_bits || e.frame_status[pd.frame]) return;
     const EncPicState &st = e.state[sd.pic];
-    const uint32_t comp[3] = {e.final_comp[3ull * s], e.final_comp[3ull * s + 1], e.final_comp[3ull * s + 2]};
-    const uint32_t qi = e.final_qi[s];
-    const uint64_t slice_bit = 8ull * (fd.out_base + st.pic_off + e.slice_off[s]);
-    const uint32_t hb = pd.header_bytes;
-    if (warp < 3) {
-        uint64_t at = slice_bit + 8ull * hb;
-        for (int c = 0; c < warp; c++) at += 8ull * comp[c];
-        uint32_t nb, off;
-        comp_layout(fd, sd.mbs, (uint32_t)warp, nb, off);
-        component_write(e.out, at, e.coef + sd.coef + off, nb, quant_table(e, pd, qi, (uint32_t)warp));
-    } else {
-        if (lane == 0) {
-            // Slice header: size << 3, quantization_index, the component
-            // sizes (the Cr size only with alpha); the table entry.
-            bool f;
-            const uint64_t total = slice_total(hb, comp, e.alpha_bytes[s], f);
-            put_field(e.out, slice_bit, hb << 3, 8);
-            put_field(e.out, slice_bit + 8, qi, 8);
-            put_field(e.out, slice_bit + 16, comp[0] & 0xFFFFu, 16);
-            put_field(e.out, slice_bit + 32, comp[1] & 0xFFFFu, 16);
-            if (hb == 8) put_field(e.out, slice_bit + 48, comp[2] & 0xFFFFu, 16);
-            const uint64_t table_bit = 8ull * (fd.out_base + st.pic_off + 8u + 2ull * (s - pd.slice_base));
-            put_field(e.out, table_bit, (uint32_t)(total & 0xFFFFu), 16);
-        }
-        if (fd.alpha_bits) {
-            const uint64_t at = slice_bit + 8ull * ((uint64_t)hb + comp[0] + comp[1] + comp[2]);
-            alpha_write(e, sd, pd, fd, scratch, at);
-        }
-    }
+    const uint32_t *c = e.final_comp + 3ull * s;
+    const uint64_t at = 8ull * (fd.out_base + st.pic_off + e.slice_off[s] + pd.header_bytes + c[0] + c[1] + c[2]);
+    alpha_write(e, sd, pd, fd, scratch[threadIdx.x >> 5], at);
 }
 
 }  // namespace
@@ -848,10 +1098,18 @@ cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// One lane per item when the batch has enough items to fill the GPU that
+// way (a lane's walk is long, so it needs the whole machine's worth of
+// them); otherwise a warp per item.
+static bool lane_mode(const EncodeLaunch &e) { return 3ull * e.n_slices >= 1024ull * (uint64_t)e.sm_count; }
+
 cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
     const uint32_t items = 3u * e.n_slices;
-    k_cost<<<(items + kCostWarps - 1) / kCostWarps, 32 * kCostWarps, 0, s>>>(e, step);
+    if (lane_mode(e))
+        k_cost<<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, step);
+    else
+        k_cost_warp<<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, step);
     return cudaGetLastError();
 }
 
@@ -861,10 +1119,15 @@ cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_cost_window(const EncodeLaunch &e, cudaStream_t s) {
+cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
-    const uint32_t items = 3u * kWindow * e.n_slices;
-    k_cost_window<<<(items + kCostWarps - 1) / kCostWarps, 32 * kCostWarps, 0, s>>>(e);
+    const uint32_t items = 3u * e.n_slices;
+    // Level 0 covers every slice; the later levels only the few candidates,
+    // so their latency is what counts.
+    if (level == 0 && lane_mode(e))
+        k_cost_window<false><<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, level);
+    else
+        k_cost_window<true><<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, level);
     return cudaGetLastError();
 }
 
@@ -884,7 +1147,13 @@ cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s) {
 
 cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
-    k_pack<<<e.n_slices, 128, 0, s>>>(e);
+    const uint32_t items = 3u * e.n_slices;
+    k_pack<<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    k_pack_headers<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);
+    if ((err = cudaGetLastError()) != cudaSuccess || !e.any_alpha) return err;
+    k_pack_alpha<<<(e.n_slices + kAlphaWarps - 1) / kAlphaWarps, 32 * kAlphaWarps, 0, s>>>(e);
     return cudaGetLastError();
 }
 

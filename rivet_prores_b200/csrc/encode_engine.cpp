@@ -278,6 +278,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     e.n_pics = (uint32_t)plan.pdesc.size();
     e.n_slices = plan.n_slices;
     e.any_alpha = plan.any_alpha;
+    e.sm_count = ctx.sm_count;
     return e;
 }
 
@@ -381,8 +382,10 @@ Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_
         PR_CUDA(launch_rc_step(e, step, s), "k_rc_step");
         if ((st = record_kernel(kt, "k_rc_step", s))) return st;
     }
-    PR_CUDA(launch_cost_window(e, s), "k_cost_window");
-    if ((st = record_kernel(kt, "k_cost_window", s))) return st;
+    for (int level = 0; level < kWindow; level++) {
+        PR_CUDA(launch_cost_window(e, level, s), "k_cost_window");
+        if ((st = record_kernel(kt, "k_cost_window", s))) return st;
+    }
     PR_CUDA(launch_shareout(e, s), "k_shareout");
     if ((st = record_kernel(kt, "k_shareout", s))) return st;
     return enqueue_tail(ctx, ws, plan, s, kt);

@@ -10,8 +10,9 @@ namespace prores {
 // Bisection steps after the probe at 224: the interval [1, 224] halves
 // (rounding up) to one value in 8 steps (src/encode.rs:700-713).
 constexpr int kProbeSteps = 9;
-// Finer quantisers costed in one pass before the share-out; deeper ones are
-// costed by the share-out itself.
+// Finer quantisers costed before the share-out (the first for every slice,
+// the next ones for the slices that could reach them); the share-out costs
+// anything else it needs itself.
 constexpr int kWindow = 4;
 // Bytes per frame-header template: 8 + a frame_header() of at most 148.
 constexpr uint32_t kHeaderSlot = 160;
@@ -58,13 +59,18 @@ struct EncPicState {
     uint64_t budget;     // bytes for the slices
     uint64_t pic_size;   // picture_size once coded
     uint64_t pic_off;    // byte offset of the picture in its frame
+    uint64_t hi_total;   // the slices' bytes at `hi`
     int32_t lo, hi;      // bisection interval
     int32_t probe_qi;    // quantiser of the pass in flight (0: none)
     int32_t hi_probe;    // the probe step whose sizes are at `hi`
+    int32_t lo_probe;    // the failed probe step at lo - 1, or -1
     int32_t fits_at_all;
     int32_t uniform;
-    int32_t pad[2];
+    int32_t pad;
 };
+
+// A window entry that was not costed (the share-out costs it if needed).
+constexpr uint32_t kNotCosted = 0xFFFFFFFFu;
 
 struct EncodeLaunch {
     const uint16_t *in;        // input planes
@@ -88,6 +94,7 @@ struct EncodeLaunch {
     uint64_t *frame_size;    // per frame
     uint32_t n_frames, n_pics, n_slices;
     int any_alpha;
+    int sm_count;
 };
 
 cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s);
@@ -95,7 +102,7 @@ cudaError_t launch_alpha_size(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s);
 cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s);
-cudaError_t launch_cost_window(const EncodeLaunch &e, cudaStream_t s);
+cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s);
 cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s);
