@@ -6,14 +6,14 @@
 //              slice that runs past picture_size.
 //   k_entropy  persistent; one lane per slice component (Y', Cb, Cr, alpha):
 //              the slice header (src/decode.rs:301-338), then the DC and
-//              run/level/sign codes of the interleaved scan (:484-540) into
-//              the coefficient scratch, or the alpha run/difference codes
-//              (:570-595) straight into the alpha plane.
-//   k_idct     one CTA per slice: inverse quantisation, the 8x8 IDCT in the
-//              crate's exact single-precision order (src/dct.rs:36-66,
+//              run/level/sign codes of the interleaved scan (:484-540) as a
+//              list of (position, value) entries, or the alpha
+//              run/difference codes (:570-595) straight into the alpha plane.
+//   k_idct     one CTA per slice: the entries placed in shared memory,
+//              inverse quantisation, the 8x8 IDCT in the crate's exact
+//              single-precision order (src/dct.rs:36-66,
 //              src/dsp/scalar.rs:8-12) and the sample conversion, stored as
-//              woven 16-byte rows (src/decode.rs:395-438); zeroes the
-//              scratch it read.
+//              woven 16-byte rows (src/decode.rs:395-438).
 //   k_status   one CTA per picture: the first failing slice component.
 //
 // The f32 arithmetic uses __fmul_rn/__fadd_rn so that nothing is contracted
@@ -131,15 +131,19 @@ __device__ __forceinline__ int read_sym(Bits &b, const uint16_t *tab, Codebook c
     return DE_OK;
 }
 
-// scanned_coefficients() of one component (src/decode.rs:484-540) into the
-// scratch in scanned order (index n of n_blocks * 64).
-__device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const uint16_t *run_tab,
+__device__ __forceinline__ uint64_t entry(uint32_t n, int32_t v) { return ((uint64_t)n << 32) | (uint32_t)v; }
+
+// scanned_coefficients() of one component (src/decode.rs:484-540): every
+// coefficient the codes give, as (scanned index, value) entries in index
+// order; `count` gets how many (also when decoding fails part-way).
+__device__ int decode_component(Bits &b, uint32_t n_blocks, uint64_t *out, uint32_t &count, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
+    count = 0;
     uint32_t sym;
     int err = read_sym(b, nullptr, kFirstDcBook, sym);
     if (err) return err;
     int32_t prev_dc = symbol_to_signed(sym);
-    out[0] = prev_dc;
+    out[count++] = entry(0, prev_dc);
     int32_t prev_diff = 3;
     for (uint32_t i = 1; i < n_blocks; i++) {
         if ((err = read_sym(b, nullptr, dc_book(prev_diff), sym))) return err;
@@ -148,7 +152,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const 
         int64_t s = (int64_t)prev_dc + diff;
         if (s > INT32_MAX || s < INT32_MIN) return DE_DC_OVERFLOW;
         prev_dc = (int32_t)s;
-        out[i] = prev_dc;
+        out[count++] = entry(i, prev_dc);
         prev_diff = diff;
     }
     const uint32_t total = n_blocks * 64;
@@ -173,7 +177,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const 
                     int32_t level = (int32_t)lvl + 1;
                     bool neg = (w2 << l2) >> 63;
                     b.pos += l1 + l2 + 1;
-                    out[n] = neg ? -level : level;
+                    out[count++] = entry(n, neg ? -level : level);
                     n += 1;
                     prev_run = run;
                     prev_level = lvl;
@@ -189,7 +193,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const 
             return err;
         prev_run = run;
         n += run;
-        if (n >= total || run >= total) return DE_RUN_PAST_END;
+        if (n >= total) return DE_RUN_PAST_END;
         if ((err = read_sym(b, level_tab + (prev_level < 8u ? prev_level : 8u) * kDecodeEntries,
                             level_book(prev_level), lvl)))
             return err;
@@ -198,7 +202,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, int32_t *out, const 
         bool neg = b.peek() >> 63;
         b.pos += 1;
         int32_t level = (int32_t)lvl + 1;
-        out[n] = neg ? -level : level;
+        out[count++] = entry(n, neg ? -level : level);
         n += 1;
     }
     return DE_OK;
@@ -275,6 +279,9 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
     const SliceDesc sd = d.slices[s];
     const PicDesc &pd = d.pics[sd.pic];
     if (d.pic_status[sd.pic].locate_slice >= 0) return;  // never read: the picture failed before decoding
+    // Every run writes every count of the slices it decodes (a failing
+    // component's too), so k_idct never reads a stale one.
+    if (comp < 3) d.coef_count[3ull * s + comp] = 0;
     const FrameDesc &fd = d.frames[pd.frame];
     const bool has_alpha = fd.alpha_bits != 0;
     if (comp == 3 && !has_alpha) {
@@ -336,7 +343,9 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
         const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
         const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
         const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
-        err = decode_component(b, n_blocks, d.coef + base, run_tab, level_tab);
+        uint32_t count = 0;
+        err = decode_component(b, n_blocks, d.coef + base, count, run_tab, level_tab);
+        d.coef_count[3ull * s + comp] = count;
     }
     *slot = make_int2(err, 0);
 }
@@ -480,7 +489,7 @@ __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_
     }
 }
 
-__global__ void __launch_bounds__(kIdctThreads) k_idct(DecodeLaunch d) {
+__global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
     extern __shared__ __align__(16) unsigned char smem[];
     int32_t *cs = reinterpret_cast<int32_t *>(smem);                   // scanned coefficients
     float *tmp = reinterpret_cast<float *>(smem + 4 * kMaxSliceCoefs);  // row pass, [v][x][blk] per component
@@ -498,12 +507,21 @@ __global__ void __launch_bounds__(kIdctThreads) k_idct(DecodeLaunch d) {
     const uint32_t total = 64u * (4u + 2u * cpm) * mbs;
     const uint32_t tid = threadIdx.x;
 
-    // Load the slice's scanned coefficients and leave the scratch zeroed.
-    int4 *g4 = reinterpret_cast<int4 *>(d.coef + sd.coef);
+    // The slice's coefficients: zero the block array, then place each
+    // component's (position, value) entries.
     int4 *s4 = reinterpret_cast<int4 *>(cs);
-    for (uint32_t i = tid; i < total / 4; i += kIdctThreads) {
-        s4[i] = g4[i];
-        g4[i] = make_int4(0, 0, 0, 0);
+    for (uint32_t i = tid; i < total / 4; i += kIdctThreads) s4[i] = make_int4(0, 0, 0, 0);
+    __syncthreads();
+    for (uint32_t c = 0; c < 3; c++) {
+        const uint32_t cap = 64u * (c == 0 ? 4u : cpm) * mbs;
+        const uint32_t start = c == 0 ? 0u : 64u * mbs * (4u + (c - 1u) * cpm);
+        const uint32_t n = min(d.coef_count[3ull * blockIdx.x + c], cap);
+        const uint64_t *list = d.coef + sd.coef + start;
+        for (uint32_t i = tid; i < n; i += kIdctThreads) {
+            const uint64_t e = __ldg(reinterpret_cast<const unsigned long long *>(list) + i);
+            const uint32_t pos = (uint32_t)(e >> 32);
+            if (pos < cap) cs[start + pos] = (int32_t)(uint32_t)e;
+        }
     }
     uint32_t qi = sd.size >= 2 ? d.bits[sd.off + 1] : 1u;
     qi = qi < 1u ? 1u : (qi > 224u ? 224u : qi);

@@ -41,7 +41,7 @@ struct PicDesc {
 // One slice, located (filled on the device from the slice table).
 struct SliceDesc {
     uint64_t off;   // byte offset of the slice in the bitstream buffer
-    uint64_t coef;  // first coefficient in the scratch (scanned order, Y' Cb Cr)
+    uint64_t coef;  // first entry of the slice's coefficient lists (Y', Cb, Cr regions)
     uint32_t size;  // bytes
     uint32_t pic;
     uint16_t mb_x, mb_y;
@@ -86,7 +86,11 @@ struct DecodeLaunch {
     SliceDesc *slices;
     int2 *slot_status;  // 4 per slice
     PicStatus *pic_status;
-    int32_t *coef;  // scratch, zero between uses
+    // Decoded coefficients, per slice component: (scanned position << 32 |
+    // value) in position order, in a region as long as the component has
+    // coefficients; coef_count[3 s + c] says how many are there.
+    uint64_t *coef;
+    uint32_t *coef_count;
     uint16_t *planes;
     uint16_t *alpha;
     const uint8_t *weights;  // [set][2][64] raster weights

@@ -284,15 +284,8 @@ Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaSt
     PR_CUDA(ws.alpha.reserve(2 * (plan.alpha_total + 8)), "cudaMalloc alpha");
     PR_CUDA(ws.weights.reserve(plan.weights.size() + 128), "cudaMalloc");
     PR_CUDA(ws.counter.reserve(64), "cudaMalloc");
-    const size_t coef_bytes = 4 * (plan.coef_total + 64);
-    if (coef_bytes > ws.coef.cap || !ws.coef.p) {
-        PR_CUDA(ws.coef.reserve(coef_bytes), "cudaMalloc coefficient scratch");
-        ws.coef_clean = false;
-    }
-    if (!ws.coef_clean) {
-        PR_CUDA(cudaMemsetAsync(ws.coef.p, 0, ws.coef.cap, s), "memset scratch");
-        ws.coef_clean = true;
-    }
+    PR_CUDA(ws.coef.reserve(8 * (plan.coef_total + 64)), "cudaMalloc coefficient lists");
+    PR_CUDA(ws.coef_count.reserve(4 * 3 * ((size_t)plan.n_slices + 1)), "cudaMalloc");
     if (!plan.fdesc.empty())
         PR_CUDA(cudaMemcpyAsync(ws.frames.p, plan.fdesc.data(), sizeof(FrameDesc) * plan.fdesc.size(),
                                 cudaMemcpyHostToDevice, s),
@@ -318,7 +311,8 @@ DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan 
     d.slices = ws.slices.as<SliceDesc>();
     d.slot_status = ws.slot_status.as<int2>();
     d.pic_status = ws.pic_status.as<PicStatus>();
-    d.coef = ws.coef.as<int32_t>();
+    d.coef = ws.coef.as<uint64_t>();
+    d.coef_count = ws.coef_count.as<uint32_t>();
     d.planes = ws.planes.as<uint16_t>();
     d.alpha = ws.alpha.as<uint16_t>();
     d.weights = ws.weights.as<uint8_t>();
@@ -578,7 +572,6 @@ int prores_decode_batch(prores_ctx *ctx, const prores_buf *in, int n, uint32_t o
     if (!st) st = fetch_decode(*ws, plan, s, out, status, &first);
     if (st) {
         cudaStreamSynchronize(s);
-        ws->coef_clean = false;
         ctx->impl.release(std::move(ws));
         return fail(st);
     }

@@ -38,12 +38,11 @@ struct PinnedBuf {
 struct Workspace {
     int device = 0;
     cudaStream_t stream = nullptr;
-    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, planes, alpha, weights, counter;
+    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter;
     // encode
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
     PinnedBuf host_stage;
-    bool coef_clean = true;  // the decode scratch is all zero
     ~Workspace();
 };
 
