@@ -49,6 +49,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=4.0, help="0 skips the serving run")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean requests/s (Poisson)")
     return ap.parse_args()
 
 
@@ -171,6 +173,7 @@ def run_b200(args):
 
     import rivet_prores_b200 as P
     from rivet_prores_b200 import workloads
+    from rivet_prores_b200.sharding import max_over_ranks
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -240,10 +243,7 @@ def run_b200(args):
     t_enc = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps))
     t_dec = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps))
     total = ev[0][0].elapsed_time(ev[-1][2])
-    if dist:
-        t = torch.tensor([total, t_enc, t_dec], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total, t_enc, t_dec = [float(x) for x in t.tolist()]
+    total, t_enc, t_dec = max_over_ranks([total, t_enc, t_dec], dist, "cuda")
     frames_done = B * args.steps * world
     value = frames_done / (total / 1000.0)
     dec_fps = frames_done / (t_dec / 1000.0)
@@ -337,10 +337,7 @@ def run_b200(args):
         e1.record(stream)
         stream.synchronize()
         t = e0.elapsed_time(e1)
-        if dist:
-            tt = torch.tensor([t], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks([t], dist, "cuda")[0]
         e2e = {"value": round(B * e2e_steps * world / (t / 1000.0), 3), "unit": "frames/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "steps": e2e_steps, "path": "prores_{encode,decode}_job_{upload,launch,fetch}, pinned host buffers"}
@@ -355,6 +352,10 @@ def run_b200(args):
         cpu = {"value": round(fps, 3), "unit": "frames/s", "cores": cores, "kind": "port",
                "sample": f"{n_cpu} UHD 422 HQ frames, encode + decode each, best of 3, oracle codec on "
                          f"{cores} threads"}
+
+    serve = None
+    if rank == 0 and args.serve_seconds > 0:
+        serve = run_serving(args, local)
 
     if dist:
         dist.barrier()
@@ -384,9 +385,47 @@ def run_b200(args):
                      "peak_source": peak_kind,
                      "algorithmic_bytes": f"{ALGO_BYTES_PER_FRAME} B per frame (packet + u16 planes) x {B}"},
         "cpu_baseline": cpu,
+        "serve": serve,
         "clocks": clock_info,
     }
     print(json.dumps(line))
+
+
+def run_serving(args, device):
+    """Poisson requests (70 % decode, 30 % encode) over the heterogeneous
+    mix, served with continuous batching under an 8 GiB device budget; then
+    the same offered load served one request per launch."""
+    import numpy as np
+
+    import rivet_prores_b200 as P
+    from rivet_prores_b200 import serve as S
+    from rivet_prores_b200 import workloads
+
+    pool = workloads.mixed_pool()
+    packets = [P.Encoder(c, device=device).encode(f) for f, c in pool]
+
+    def maker(seed):
+        rng = np.random.Generator(np.random.PCG64(seed))
+
+        def make(i):
+            k = int(rng.integers(len(pool)))
+            if rng.random() < 0.7:
+                return ("decode", packets[k])
+            return ("encode", pool[k][0], pool[k][1])
+        return make
+
+    out = {"mix": "720x486i HQ, 720p LT, 1080p Proxy/422/HQ, UHD HQ, 4096x2160 4444 (16-bit in); 70/30 decode/encode",
+           "budget_bytes": 8 << 30}
+    for name, workers, max_batch, seconds in [("batched", 3, 64, args.serve_seconds),
+                                              ("plain", 1, 1, max(1.0, args.serve_seconds / 4))]:
+        srv = S.Server(memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
+        S.poisson_run(srv, maker(1), rate=200.0, seconds=0.3)  # workspaces allocated, not measured
+        srv.close()
+        srv = S.Server(memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
+        st = S.poisson_run(srv, maker(2), rate=args.serve_rate, seconds=seconds)
+        srv.close()
+        out[name] = st
+    return out
 
 
 def main():

@@ -1,0 +1,239 @@
+"""Serving: continuous batching of decode and encode requests on one GPU.
+
+Requests arrive at any time (`submit_decode`, `submit_encode`, each a
+Future). Worker threads each take the oldest waiting request's kind and as
+many further requests of that kind, oldest first, as the device-memory
+budget admits. Each batch is one launch into the library (`decode_batch` /
+`encode_batch`). Requests that arrive while other batches run are admitted
+as workers and memory free up, and their batches run on the device
+alongside the others: each call has its own workspace and stream, and the
+library releases the GIL while it runs. Every result is the one the request
+would get alone; the library's output never depends on the batch.
+
+The memory estimate per frame covers what a batch keeps on the device:
+for decode the bitstream, the coefficient lists (8 B a coefficient) and the
+planes; for encode the planes in, the f32 coefficients and the packet
+region.
+"""
+
+from __future__ import annotations
+
+import collections
+import ctypes
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Callable, Deque, List, Optional
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    kind: str  # "decode" or "encode"
+    payload: object  # bytes for decode, Frame for encode
+    config: object = None  # encode Config
+    bit_depth: Optional[int] = None
+    cost: int = 0  # device bytes while in flight
+    t_submit: float = 0.0
+    t_done: float = 0.0
+    future: Future = field(default_factory=Future)
+
+
+def decode_cost(data: bytes) -> int:
+    """Device bytes a decode of `data` holds: bitstream, lists, planes."""
+    from . import _abi
+
+    info = _abi.Frame_()
+    if _abi.lib().prores_probe(data, len(data), 0, ctypes.byref(info)) != _abi.OK:
+        return len(data) + 4096
+    return len(data) + 10 * info.data_len + 2 * info.alpha_len + 4096
+
+
+def encode_cost(frame, config) -> int:
+    """Device bytes an encode of `frame` holds: planes in, f32 coefficients,
+    the packet region."""
+    n = int(frame.data.size)
+    target = config.target_frame_bytes or config.profile.target_frame_bytes(frame.width, frame.height)
+    alpha = 0 if frame.alpha is None else 4 * frame.alpha.size
+    return 6 * n + int(target) + alpha + 4096
+
+
+class GpuBackend:
+    """The library's batched calls."""
+
+    def __init__(self, device: int = 0):
+        from . import Decoder, Encoder
+
+        self.device = device
+        self._Decoder = Decoder
+        self._Encoder = Encoder
+
+    def decode(self, reqs: List[Request]):
+        by_depth = collections.defaultdict(list)
+        for i, r in enumerate(reqs):
+            by_depth[r.bit_depth].append(i)
+        out = [None] * len(reqs)
+        for depth, idx in by_depth.items():
+            res = self._Decoder(bit_depth=depth, device=self.device).decode_batch([reqs[i].payload for i in idx])
+            for i, r in zip(idx, res):
+                out[i] = r
+        return out
+
+    def encode(self, reqs: List[Request]):
+        frames = [r.payload for r in reqs]
+        configs = [r.config for r in reqs]
+        return self._Encoder(configs[0], device=self.device).encode_batch(frames, configs)
+
+
+class Server:
+    """Continuous batching over `backend` (GpuBackend by default).
+
+    memory_budget: device bytes all in-flight batches may hold together.
+    max_batch: frames per batch. workers: batches in flight at once.
+    """
+
+    def __init__(self, backend=None, memory_budget: int = 8 << 30, max_batch: int = 64, workers: int = 2,
+                 device: int = 0):
+        self.backend = backend if backend is not None else GpuBackend(device)
+        self.budget = memory_budget
+        self.max_batch = max_batch
+        self.in_use = 0
+        self.queue: Deque[Request] = collections.deque()
+        self.cv = threading.Condition()
+        self.closed = False
+        self.done: List[Request] = []
+        self.batches: List[int] = []
+        self.peak_in_use = 0
+        self.threads = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
+        for t in self.threads:
+            t.start()
+
+    # -------------------------------------------------------------- intake
+
+    def submit_decode(self, data: bytes, bit_depth: Optional[int] = None, cost: Optional[int] = None) -> Future:
+        data = bytes(data)
+        r = Request("decode", data, None, bit_depth, decode_cost(data) if cost is None else cost)
+        return self._submit(r)
+
+    def submit_encode(self, frame, config, cost: Optional[int] = None) -> Future:
+        r = Request("encode", frame, config, None, encode_cost(frame, config) if cost is None else cost)
+        return self._submit(r)
+
+    def _submit(self, r: Request) -> Future:
+        r.t_submit = time.perf_counter()
+        with self.cv:
+            if self.closed:
+                raise RuntimeError("server closed")
+            self.queue.append(r)
+            self.cv.notify_all()
+        return r.future
+
+    # -------------------------------------------------------------- batching
+
+    def _take(self) -> List[Request]:
+        """Under the lock: the oldest request's kind, and further requests of
+        that kind oldest first, while the budget admits them. A request larger
+        than the whole budget runs alone once nothing else is in flight."""
+        head = self.queue[0]
+        batch, cost = [], 0
+        free = self.budget - self.in_use
+        for r in list(self.queue):
+            if r.kind != head.kind:
+                continue
+            if len(batch) >= self.max_batch:
+                break
+            if cost + r.cost > free and not (not batch and self.in_use == 0):
+                break
+            batch.append(r)
+            cost += r.cost
+        for r in batch:
+            self.queue.remove(r)
+        self.in_use += cost
+        self.peak_in_use = max(self.peak_in_use, self.in_use)
+        return batch
+
+    def _worker(self):
+        while True:
+            with self.cv:
+                while True:
+                    if self.closed and not self.queue:
+                        return
+                    if self.queue:
+                        batch = self._take()
+                        if batch:
+                            break
+                    self.cv.wait(0.05)
+            try:
+                results = self.backend.decode(batch) if batch[0].kind == "decode" else self.backend.encode(batch)
+                exc = None
+            except Exception as e:  # a device failure fails the batch, not the server
+                results, exc = None, e
+            now = time.perf_counter()
+            with self.cv:
+                self.in_use -= sum(r.cost for r in batch)
+                self.batches.append(len(batch))
+                for i, r in enumerate(batch):
+                    r.t_done = now
+                    self.done.append(r)
+                self.cv.notify_all()
+            for i, r in enumerate(batch):
+                if exc is not None:
+                    r.future.set_exception(exc)
+                else:
+                    r.future.set_result(results[i])
+
+    def close(self):
+        with self.cv:
+            self.closed = True
+            self.cv.notify_all()
+        for t in self.threads:
+            t.join()
+
+    # -------------------------------------------------------------- metrics
+
+    def stats(self) -> dict:
+        with self.cv:
+            lat = sorted((r.t_done - r.t_submit) * 1000.0 for r in self.done)
+            batches = list(self.batches)
+            first = min((r.t_submit for r in self.done), default=0.0)
+            last = max((r.t_done for r in self.done), default=0.0)
+        if not lat:
+            return {"requests": 0}
+        pct = lambda p: lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
+        return {"requests": len(lat), "p50_ms": round(pct(50), 3), "p99_ms": round(pct(99), 3),
+                "max_ms": round(lat[-1], 3), "frames_per_s": round(len(lat) / max(last - first, 1e-9), 2),
+                "batches": len(batches), "mean_batch": round(float(np.mean(batches)), 2),
+                "peak_device_bytes_admitted": self.peak_in_use}
+
+
+def poisson_run(server: Server, make_request: Callable[[int], tuple], rate: float, seconds: float,
+                seed: int = 0) -> dict:
+    """Submits requests at Poisson times (mean `rate` per second) for
+    `seconds`; make_request(i) gives ("decode", data) or ("encode", frame,
+    config). Waits for all and returns the server's stats."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    futures = []
+    t0 = time.perf_counter()
+    t = 0.0
+    i = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        delay = t0 + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        req = make_request(i)
+        if req[0] == "decode":
+            futures.append(server.submit_decode(req[1]))
+        else:
+            futures.append(server.submit_encode(req[1], req[2]))
+        i += 1
+    for f in futures:
+        f.result()
+    s = server.stats()
+    s["offered_rate"] = rate
+    s["seconds"] = seconds
+    return s

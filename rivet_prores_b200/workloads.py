@@ -86,3 +86,25 @@ def uhd_422_hq(n: int, config: int = 1, unique: Optional[int] = None) -> List[Fr
 
 def hq_config() -> Config:
     return Config(Profile.Hq)
+
+
+def mixed_pool(seed_base: int = 3000):
+    """One frame of each kind in the heterogeneous mix: 720x486 interlaced 422
+    HQ, 1280x720 LT, 1920x1080 Proxy / 422 / HQ, 3840x2160 HQ and 4096x2160
+    4444 from 16-bit input; slice widths drawn from {1, 2, 4, 8} macroblocks.
+    Returns [(frame, config)]."""
+    rng = np.random.Generator(np.random.PCG64([seed_base, 99]))
+    kinds = [
+        (720, 486, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.BottomFieldFirst),
+        (1280, 720, ChromaFormat.Yuv422, 10, Profile.Lt, Interlace.Progressive),
+        (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Proxy, Interlace.Progressive),
+        (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Standard, Interlace.Progressive),
+        (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.Progressive),
+        (3840, 2160, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.Progressive),
+        (4096, 2160, ChromaFormat.Yuv444, 16, Profile.P4444, Interlace.Progressive),
+    ]
+    out = []
+    for i, (w, h, chroma, depth, profile, interlace) in enumerate(kinds):
+        f = picture(w, h, chroma, depth, seed_base + i, interlace=interlace)
+        out.append((f, Config(profile, log2_slice_mbs=int(rng.integers(0, 4)))))
+    return out
