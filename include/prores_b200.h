@@ -165,6 +165,34 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
 
 void prores_buffer_free(void *p);
 
+/* ---- decode without device allocation --------------------------------- */
+
+/* Size of the fixed device array prores_decode_noalloc keeps its scratch in:
+ * enough for any frame up to 1920x1080, 4:2:2 or 4:4:4. */
+#define PRORES_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* Decodes one frame, like prores_decode, without allocating any device
+ * memory. It has no counterpart in the reference crate. It is for callers
+ * that cannot allocate while they decode: a real-time playback thread (a
+ * cudaMalloc can stall it, and cudaFree waits for the whole device), or a
+ * host application whose device memory all comes from its own pool
+ * allocator, which an allocation outside the pool would break. The caller
+ * passes the frame's bytes in host memory and device buffers for the output
+ * (d_planes: Y'‖Cb‖Cr, planes_len samples; d_alpha: the alpha plane, NULL
+ * for a frame without alpha; prores_probe gives both sizes). The decoder's
+ * scratch lives in one static device array of PRORES_NOALLOC_SCRATCH_BYTES
+ * that every GPU which loads it holds until the process exits; a frame that
+ * needs more (larger than 1920x1080) is refused with PRORES_CONFIG. No
+ * context is needed: the first call on a device sets that device up (the
+ * array's address, the kernels' settings, the decoder's tables), so make that
+ * first call before any stream capture. Every call shares the one array; the
+ * call resets what must start at zero and returns after `stream` (a
+ * cudaStream_t, or NULL) has finished, and calls whose work overlaps on the
+ * GPU (from several threads or streams at once) race and must not be made. */
+int prores_decode_noalloc(int device, const uint8_t *data, size_t len, uint32_t out_bit_depth,
+                          uint16_t *d_planes, size_t planes_len, uint16_t *d_alpha, size_t alpha_len,
+                          void *stream);
+
 /* ---- resident jobs (batching and serving) ----------------------------- */
 
 /* A decode job keeps a batch's bitstreams and planes resident in device
