@@ -48,6 +48,7 @@ def parse_args():
     ap.add_argument("--unique", type=int, default=4, help="distinct synthetic pictures in a batch")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-chunks", type=int, default=4, help="streams the end-to-end batch is split over")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="0 skips the serving run")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean requests/s (Poisson)")
@@ -300,48 +301,85 @@ def run_b200(args):
 
     # End to end through the C ABI with host buffers: each step copies the
     # frames in from pinned memory, encodes, reads the packets back, copies
-    # them in, decodes and reads the planes back.
+    # them in, decodes and reads the planes back. The batch goes through in
+    # chunks, each on its own stream and host thread, so that one chunk's
+    # copies overlap another's kernels and both copy directions run at once.
     e2e = None
     if not args.no_e2e:
+        import concurrent.futures as cf
+
         n_samples = frames[0].data.size
         host = torch.empty((B, n_samples), dtype=torch.uint16, pin_memory=True).numpy()
-        hframes = []
-        for i, f in enumerate(frames):
-            host[i] = f.data
-            g = P.Frame(f.width, f.height, f.bit_depth, f.chroma, f.interlace, f.metadata, host[i], f.planes, None)
-            hframes.append(g)
         out_host = torch.empty((B, n_samples), dtype=torch.uint16, pin_memory=True).numpy()
-        arrays = [(out_host[i], None) for i in range(B)]
-        e2e_steps = max(2, args.steps // 2)
+        chunks = max(1, min(args.e2e_chunks, B))
+        bounds = [(c * B // chunks, (c + 1) * B // chunks) for c in range(chunks)]
+        lanes = []
+        for lo, hi in bounds:
+            hframes = []
+            for i in range(lo, hi):
+                host[i] = frames[i].data
+                f = frames[i]
+                hframes.append(P.Frame(f.width, f.height, f.bit_depth, f.chroma, f.interlace, f.metadata, host[i],
+                                       f.planes, None))
+            cenc = P.EncodeJob(hframes, cfg, device=local)
+            cdec = P.DecodeJob(packets[lo:hi], device=local)
+            lanes.append({"enc": cenc, "dec": cdec, "frames": hframes, "stream": torch.cuda.Stream(),
+                          "arrays": [(out_host[i], None) for i in range(lo, hi)]})
 
-        def e2e_step():
-            enc.upload(hframes, stream)
-            enc.launch(stream, graph=True)
-            pk = enc.fetch(stream, copy=False)
-            dec.upload([np.frombuffer(p, dtype=np.uint8) for p in pk], stream)
-            dec.launch(stream, graph=True)
-            res = dec.fetch(stream, arrays)
+        def lane_step(lane):
+            st = lane["stream"]
+            lane["enc"].upload(lane["frames"], st)
+            lane["enc"].launch(st, graph=True)
+            pk = lane["enc"].fetch(st, copy=False)
+            lane["dec"].upload([np.frombuffer(p, dtype=np.uint8) for p in pk], st)
+            lane["dec"].launch(st, graph=True)
+            res = lane["dec"].fetch(st, lane["arrays"])
+            lane["end"].record(st)
             return pk, res
 
+        pool = cf.ThreadPoolExecutor(max_workers=chunks)
+        main = torch.cuda.Stream()
+
+        def e2e_step():
+            start = torch.cuda.Event(enable_timing=True)
+            start.record(main)
+            for lane in lanes:
+                lane["stream"].wait_event(start)
+                lane["end"] = torch.cuda.Event(enable_timing=True)
+            outs = list(pool.map(lane_step, lanes))
+            for lane in lanes:
+                main.wait_event(lane["end"])
+            end = torch.cuda.Event(enable_timing=True)
+            end.record(main)
+            return start, end, outs
+
         for _ in range(2):
-            pk, res = e2e_step()
-        h2d = sum(2 * f.data.size for f in frames) + sum(len(p) for p in pk)
-        d2h = sum(len(p) for p in pk) + sum(2 * a.size for a, _ in arrays)
+            e2e_step()
+        main.synchronize()
+        e2e_steps = max(2, args.steps // 2)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(e2e_steps):
-            e2e_step()
-        e1.record(stream)
-        stream.synchronize()
-        t = e0.elapsed_time(e1)
+        marks = [e2e_step() for _ in range(e2e_steps)]
+        main.synchronize()
+        t = marks[0][0].elapsed_time(marks[-1][1])
+        outs = marks[-1][2]
+        pk = [p for o in outs for p in o[0]]
+        res = [r for o in outs for r in o[1]]
+        h2d = sum(2 * f.data.size for f in frames) + sum(len(p) for p in pk)
+        d2h = sum(len(p) for p in pk) + sum(2 * out_host[i].size for i in range(B))
         t = max_over_ranks([t], dist, "cuda")[0]
         e2e = {"value": round(B * e2e_steps * world / (t / 1000.0), 3), "unit": "frames/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "steps": e2e_steps, "path": "prores_{encode,decode}_job_{upload,launch,fetch}, pinned host buffers"}
-        assert np.array_equal(res[0].data, dec.fetch(stream)[0].data)
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+               "path": f"prores_{{encode,decode}}_job_{{upload,launch,fetch}}, pinned host buffers, "
+                       f"{chunks} chunks on their own streams"}
+        for i, r in enumerate(res):
+            assert np.array_equal(r.data, out_host[i])
+        assert np.array_equal(out_host[0], dec.fetch(stream)[0].data)
+        pool.shutdown()
+        for lane in lanes:
+            lane["enc"].close()
+            lane["dec"].close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
