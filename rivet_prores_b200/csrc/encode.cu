@@ -357,33 +357,68 @@ __device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, f
     return bits;
 }
 
-// Bits of one quantised component (src/encode.rs:398-409), one lane: the
-// crate's own walk over the scanned positions, four coefficients a load.
-__device__ uint32_t lane_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
+// One AC position of a lane's walk: x = F inv, m = floor(|x| + 0.42)
+// (src/dsp/scalar.rs:19-39), tested for zero in float; only a non-zero
+// coefficient is converted and coded (its run from the last one, its level,
+// both by context).
+struct AcWalk {
+    uint32_t prev_run = 4, prev_level = 1, pos = 0;
+};
+
+template <class Emit>
+__device__ __forceinline__ void ac_position(AcWalk &w, float f, float inv, uint32_t p, Emit emit) {
+    const float x = __fmul_rn(f, inv);
+    const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
+    if (m >= 1.0f) {
+        const uint32_t run = p - w.pos;
+        const uint32_t level = (uint32_t)__float2int_rz(m) - 1u;
+        emit(w, run, level, x < 0.0f);
+        w.prev_run = run;
+        w.prev_level = level;
+        w.pos = p + 1;
+    }
+}
+
+// Walks a component's AC positions (n_blocks onwards), four coefficients a
+// load; with two blocks a load spans two scan positions.
+template <class Emit>
+__device__ __forceinline__ void ac_walk(const float *f, uint32_t n_blocks, const float *inv, Emit emit) {
     const uint32_t total = 64u * n_blocks;
     const uint32_t shift = 31u - __clz(n_blocks);
-    uint32_t bits = dc_bits(f, n_blocks, __ldg(inv));
-    uint32_t prev_run = 4, prev_level = 1, pos = n_blocks;
-    for (uint32_t p0 = n_blocks & ~3u; p0 < total; p0 += 4) {
-        const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
-        const float vv[4] = {v.x, v.y, v.z, v.w};
-        const uint32_t s0 = p0 >> shift;
-        const float inv_a = __ldg(inv + s0), inv_b = __ldg(inv + min(s0 + 1u, 63u));
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t p = p0 + j;
-            if (p < n_blocks) continue;
-            const int32_t q = quantise1(vv[j], ((p >> shift) == s0) ? inv_a : inv_b, kAcRounding);
-            if (q != 0) {
-                const uint32_t run = p - pos;
-                const uint32_t level = (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u;
-                bits += t.run_len(prev_run, run) + t.level_len(prev_level, level) + 1u;
-                prev_run = run;
-                prev_level = level;
-                pos = p + 1;
+    AcWalk w;
+    w.pos = n_blocks;
+    if (n_blocks >= 4) {
+        for (uint32_t p0 = n_blocks; p0 < total; p0 += 4) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+            const float iv = __ldg(inv + (p0 >> shift));
+            ac_position(w, v.x, iv, p0, emit);
+            ac_position(w, v.y, iv, p0 + 1, emit);
+            ac_position(w, v.z, iv, p0 + 2, emit);
+            ac_position(w, v.w, iv, p0 + 3, emit);
+        }
+    } else {
+        // Two blocks: positions 0 and 1 are the DCs; p and p + 1 share scan
+        // position p / 2.
+        for (uint32_t p0 = 0; p0 < total; p0 += 4) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+            const float ia = __ldg(inv + (p0 >> 1)), ib = __ldg(inv + (p0 >> 1) + 1);
+            if (p0 > 0) {
+                ac_position(w, v.x, ia, p0, emit);
+                ac_position(w, v.y, ia, p0 + 1, emit);
             }
+            ac_position(w, v.z, ib, p0 + 2, emit);
+            ac_position(w, v.w, ib, p0 + 3, emit);
         }
     }
+}
+
+// Bits of one quantised component (src/encode.rs:398-409), one lane: the
+// crate's own walk over the scanned positions.
+__device__ uint32_t lane_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
+    uint32_t bits = dc_bits(f, n_blocks, __ldg(inv));
+    ac_walk(f, n_blocks, inv, [&](const AcWalk &w, uint32_t run, uint32_t level, bool) {
+        bits += t.run_len(w.prev_run, run) + t.level_len(w.prev_level, level) + 1u;
+    });
     return bits;
 }
 
@@ -670,14 +705,75 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
     }
 }
 
-// The share-out (src/encode.rs:769-793), one warp per picture. With
-// D = remaining_budget - remaining_base, slice i steps from the uniform
-// quantiser to the next finer one while that size n fits and
-// n <= base + floor(D mbs / remaining_mbs), i.e. while n <= base or
-// D >= ceil((n - base) remaining_mbs / mbs); D then falls by what the slice
-// took over its base. Each lane works out its slice's thresholds; the walk
-// itself only compares D with them, 32 slices at a time by ballot, and
-// costs a deeper quantiser with the warp when a slice gets that far.
+// The share-out (src/encode.rs:769-793). With D = remaining_budget -
+// remaining_base, slice i steps from the uniform quantiser to the next finer
+// one while that size n fits and n <= base + floor(D mbs / remaining_mbs),
+// i.e. while n <= base or D >= ceil((n - base) remaining_mbs / mbs); D then
+// falls by what the slice took over its base. Three kernels:
+//   k_share_prep   every slice in parallel: its base and, for each window
+//                  level, the threshold on D and the size over the base;
+//   k_shareout     one warp per picture, the only serial part: D against
+//                  the thresholds, 32 slices at a time by ballot, each
+//                  stepping slice settled by its own lane; the warp costs a
+//                  deeper quantiser together when a slice gets past the
+//                  window;
+//   k_share_final  every slice in parallel: its quantiser and sizes.
+constexpr uint32_t kDeepFlag = 0x80000000u;  // share_steps: sizes are in final_comp already
+
+__global__ void k_share_prep(EncodeLaunch e) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= e.n_slices) return;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicState st = e.state[sd.pic];
+    SharePrep pr{};
+    if (st.uniform > 1 && st.fits_at_all) {
+        const EncPicDesc &pd = e.pics[sd.pic];
+        const uint32_t hb = pd.header_bytes, alpha = e.alpha_bytes[s];
+        const uint32_t *u = e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u;
+        const uint32_t uc[3] = {u[0], u[1], u[2]};
+        bool f;
+        const uint64_t base = slice_total(hb, uc, alpha, f);
+        const uint64_t rem = mbs_from(pd, sd);
+        const uint32_t shift = 31u - __clz(sd.mbs);
+        pr.base = (uint32_t)base;
+#pragma unroll
+        for (int j = 0; j < kWindow; j++) {
+            pr.thr[j] = ~0ull;
+            if (st.uniform - j <= 1) continue;
+            const uint32_t *c = level_comp(e, st, (uint32_t)j, s);
+            if (c[0] == kNotCosted) continue;  // unknown: the walk costs it if reached
+            const uint32_t cc[3] = {c[0], c[1], c[2]};
+            bool fits;
+            const uint64_t n = slice_total(hb, cc, alpha, fits);
+            pr.known |= 1u << j;
+            pr.delta[j] = (int32_t)((int64_t)n - (int64_t)base);
+            if (fits) pr.thr[j] = n <= base ? 0ull : ((((n - base) * rem) + sd.mbs - 1) >> shift);
+        }
+    }
+    e.share_prep[s] = pr;
+}
+
+// Steps a slice takes at D through its known levels (the walk of
+// src/encode.rs:776-788 while the sizes are known), and whether it then
+// needs a level nobody costed (`deep`).
+__device__ __forceinline__ uint32_t steps_at(const SharePrep &p, uint64_t D, int32_t uniform, bool &deep) {
+    deep = false;
+    uint32_t k = 0;
+#pragma unroll
+    for (int j = 0; j < kWindow; j++) {
+        // k == j steps so far: the quantiser is uniform - j.
+        if (uniform - j <= 1) return k;
+        if (!((p.known >> j) & 1u)) {
+            deep = true;
+            return k;
+        }
+        if (D < p.thr[j]) return k;
+        k++;
+    }
+    deep = uniform - kWindow > 1;
+    return k;
+}
+
 constexpr int kShareWarps = 4;
 
 __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
@@ -689,135 +785,94 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     const int lane = threadIdx.x & 31;
     const EncPicDesc pd = e.pics[p];
     const EncPicState st = e.state[p];
-    const EncFrameDesc &fd = e.frames[pd.frame];
-    const uint32_t *used_c = e.probe_comp + (uint64_t)st.hi_probe * e.n_slices * 3u;
-    const uint32_t hb = pd.header_bytes;
     const bool refine = st.uniform > 1 && st.fits_at_all;
-    uint64_t D = refine ? st.budget - st.hi_total : 0;
+    if (!refine) {
+        for (uint32_t k = lane; k < pd.n_slices; k += 32) e.share_steps[pd.slice_base + k] = 0;
+        return;
+    }
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const uint32_t hb = pd.header_bytes;
+    uint64_t D = st.budget - st.hi_total;
+    SharePrep next{};
+    if ((uint32_t)lane < pd.n_slices) next = e.share_prep[pd.slice_base + lane];
     for (uint32_t k0 = 0; k0 < pd.n_slices; k0 += 32) {
+        const SharePrep mine = next;
         const uint32_t k = k0 + lane;
         const bool live = k < pd.n_slices;
-        const uint32_t s = pd.slice_base + (live ? k : 0u);
-        uint32_t base_c[3] = {0, 0, 0}, alpha = 0, mbs = 1, shift = 0;
-        uint64_t base = 0, rem = 1;
-        uint64_t thr[kWindow];
-        uint64_t size[kWindow];
-        bool ok[kWindow];
-        if (live) {
-            const EncSliceDesc sd = e.slices[s];
-            base_c[0] = used_c[3ull * s];
-            base_c[1] = used_c[3ull * s + 1];
-            base_c[2] = used_c[3ull * s + 2];
-            alpha = e.alpha_bytes[s];
-            mbs = sd.mbs;
-            shift = 31u - __clz(mbs);
-            rem = mbs_from(pd, sd);
-            bool f;
-            base = slice_total(hb, base_c, alpha, f);
-        }
+        // The next chunk's thresholds, fetched while this chunk is walked.
+        if (k + 32 < pd.n_slices) next = e.share_prep[pd.slice_base + k + 32];
+        uint32_t my_steps = 0;
+        uint32_t done = 0;
+        while (done < 32u) {
+            bool deep;
+            const uint32_t ks = live ? steps_at(mine, D, st.uniform, deep) : 0u;
+            const bool stepping = live && lane >= (int)done && (ks > 0 || deep);
+            const uint32_t mask = __ballot_sync(0xffffffffu, stepping);
+            if (!mask) break;
+            const uint32_t f = __ffs(mask) - 1;
+            const uint32_t fk = __shfl_sync(0xffffffffu, ks, f);
+            const bool fdeep = __shfl_sync(0xffffffffu, deep, f);
+            int64_t delta = fk ? (int64_t)__shfl_sync(0xffffffffu, mine.delta[0], f) : 0;
 #pragma unroll
-        for (int j = 0; j < kWindow; j++) {
-            ok[j] = false;
-            size[j] = 0;
-            thr[j] = ~0ull;
-            if (!(live && refine) || st.uniform - j <= 1) continue;
-            const uint32_t *c = level_comp(e, st, (uint32_t)j, s);
-            if (c[0] == kNotCosted) continue;  // unknown: costed below if reached
-            const uint32_t cc[3] = {c[0], c[1], c[2]};
-            bool fits;
-            size[j] = slice_total(hb, cc, alpha, fits);
-            ok[j] = true;
-            // Known, but never taken when it does not fit.
-            thr[j] = !fits ? ~0ull : (size[j] <= base ? 0ull : (((size[j] - base) * rem + mbs - 1) >> shift));
-        }
-        uint32_t my_qi = (uint32_t)st.uniform, my_steps = 0;
-        uint32_t deep_c[3] = {0, 0, 0};
-        if (refine) {
-            uint32_t done = 0;  // lanes below this have been walked
-            while (done < 32u && k0 + done < pd.n_slices) {
-                // The first slice from `done` on that steps at all, at this D
-                // (its first level unknown counts as "might").
-                const bool steps = live && lane >= (int)done && (!ok[0] ? st.uniform > 1 : D >= thr[0]);
-                const uint32_t mask = __ballot_sync(0xffffffffu, steps);
-                if (!mask) break;
-                const uint32_t f = __ffs(mask) - 1;
-                // Walk slice f with the whole warp: its allowed size is fixed
-                // while it steps, so every finer quantiser is a separate test.
-                const uint64_t fbase = __shfl_sync(0xffffffffu, base, f);
-                const uint32_t fmbs = __shfl_sync(0xffffffffu, mbs, f);
-                const uint64_t frem = __shfl_sync(0xffffffffu, rem, f);
-                const uint32_t falpha = __shfl_sync(0xffffffffu, alpha, f);
-                const uint64_t allowed = fbase + D * fmbs / frem;
-                int32_t qi = st.uniform;
-                uint64_t used = fbase;
-                uint32_t stepsf = 0;
-                bool stop = false, deep = false;
-                uint32_t dc[3] = {0, 0, 0};
-#pragma unroll
-                for (int jj = 0; jj < kWindow; jj++) {
-                    if (stop || qi <= 1) break;
-                    const bool known = __shfl_sync(0xffffffffu, ok[jj], f);
-                    if (!known) break;
-                    const uint64_t n = __shfl_sync(0xffffffffu, size[jj], f);
-                    const bool fits = __shfl_sync(0xffffffffu, thr[jj], f) != ~0ull;
-                    if (!(fits && n <= allowed)) {
-                        stop = true;
-                        break;
-                    }
-                    qi -= 1;
-                    used = n;
-                    stepsf++;
-                }
-                // Deeper: the warp costs quantiser qi - 1, a component at a
-                // time, and the slice steps while it fits its allowance.
-                const EncSliceDesc fsd = e.slices[pd.slice_base + k0 + f];
-                while (!stop && qi > 1) {
-                    uint32_t c3[3];
-                    for (uint32_t c = 0; c < 3; c++) c3[c] = warp_component_bytes(e, fsd, pd, fd, c, (uint32_t)(qi - 1), t);
+            for (int j = 1; j < kWindow; j++)
+                if ((uint32_t)j == fk - 1) delta = __shfl_sync(0xffffffffu, mine.delta[j], f);
+            uint32_t steps = fk;
+            if (fdeep) {
+                // Past the window: the warp costs quantiser qi - 1 and the
+                // slice steps while it fits its allowance (fixed during the
+                // slice's walk).
+                const uint32_t s = pd.slice_base + k0 + f;
+                const EncSliceDesc fsd = e.slices[s];
+                const uint32_t fbase = __shfl_sync(0xffffffffu, mine.base, f);
+                const uint32_t alpha = e.alpha_bytes[s];
+                const uint64_t allowed = fbase + D * fsd.mbs / mbs_from(pd, fsd);
+                uint32_t c3[3] = {0, 0, 0};
+                int32_t qi = st.uniform - (int32_t)fk;
+                bool any = false;
+                while (qi > 1) {
+                    uint32_t n3[3];
+                    for (uint32_t c = 0; c < 3; c++) n3[c] = warp_component_bytes(e, fsd, pd, fd, c, (uint32_t)(qi - 1), t);
                     bool fits;
-                    const uint64_t n = slice_total(hb, c3, falpha, fits);
+                    const uint64_t n = slice_total(hb, n3, alpha, fits);
                     if (!(fits && n <= allowed)) break;
                     qi -= 1;
-                    used = n;
-                    stepsf++;
-                    dc[0] = c3[0];
-                    dc[1] = c3[1];
-                    dc[2] = c3[2];
-                    deep = true;
+                    steps++;
+                    delta = (int64_t)n - (int64_t)fbase;
+                    c3[0] = n3[0];
+                    c3[1] = n3[1];
+                    c3[2] = n3[2];
+                    any = true;
                 }
-                if (lane == (int)f) {
-                    my_qi = (uint32_t)qi;
-                    my_steps = stepsf;
-                    if (deep) {
-                        deep_c[0] = dc[0];
-                        deep_c[1] = dc[1];
-                        deep_c[2] = dc[2];
-                        my_steps |= 0x80000000u;  // sizes in deep_c
-                    }
+                if (any && lane == 0) {
+                    e.final_comp[3ull * s] = c3[0];
+                    e.final_comp[3ull * s + 1] = c3[1];
+                    e.final_comp[3ull * s + 2] = c3[2];
+                    steps |= kDeepFlag;
                 }
-                D = D + fbase - used;
-                done = f + 1;
+                steps = __shfl_sync(0xffffffffu, steps, 0);
             }
+            if (lane == (int)f) my_steps = steps;
+            D = (uint64_t)((int64_t)D - delta);
+            done = f + 1;
         }
-        if (live) {
-            e.final_qi[s] = my_qi;
-            uint32_t c3[3] = {base_c[0], base_c[1], base_c[2]};
-            const uint32_t nsteps = my_steps & 0x7FFFFFFFu;
-            if (my_steps & 0x80000000u) {
-                c3[0] = deep_c[0];
-                c3[1] = deep_c[1];
-                c3[2] = deep_c[2];
-            } else if (nsteps > 0) {
-                const uint32_t *c = level_comp(e, st, nsteps - 1u, s);
-                c3[0] = c[0];
-                c3[1] = c[1];
-                c3[2] = c[2];
-            }
-            e.final_comp[3ull * s] = c3[0];
-            e.final_comp[3ull * s + 1] = c3[1];
-            e.final_comp[3ull * s + 2] = c3[2];
-        }
+        if (live) e.share_steps[pd.slice_base + k] = my_steps;
     }
+}
+
+__global__ void k_share_final(EncodeLaunch e) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= e.n_slices) return;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicState st = e.state[sd.pic];
+    const uint32_t steps = e.share_steps[s];
+    const uint32_t n = steps & ~kDeepFlag;
+    e.final_qi[s] = (uint32_t)st.uniform - n;
+    if (steps & kDeepFlag) return;  // written by the walk
+    const uint32_t *c = n == 0 ? e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u
+                               : level_comp(e, st, n - 1u, s);
+    e.final_comp[3ull * s] = c[0];
+    e.final_comp[3ull * s + 1] = c[1];
+    e.final_comp[3ull * s + 2] = c[2];
 }
 
 // ---------------------------------------------------------------- layout
@@ -963,8 +1018,6 @@ struct BitOut {
 // One quantised component's codes (src/encode.rs:413-437), one lane.
 __device__ void lane_component_write(BitOut &w, const float *f, uint32_t n_blocks, const float *inv,
                                      const LenTables &t) {
-    const uint32_t total = 64u * n_blocks;
-    const uint32_t shift = 31u - __clz(n_blocks);
     const float inv0 = __ldg(inv);
     int32_t prev_dc = 0, prev_diff = 3;
     for (uint32_t i = 0; i < n_blocks; i++) {
@@ -983,35 +1036,18 @@ __device__ void lane_component_write(BitOut &w, const float *f, uint32_t n_block
         w.put_long(cb_bits(cb, sym), cb_len(cb, sym));
         prev_dc = q;
     }
-    uint32_t prev_run = 4, prev_level = 1, pos = n_blocks;
-    for (uint32_t p0 = n_blocks & ~3u; p0 < total; p0 += 4) {
-        const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
-        const float vv[4] = {v.x, v.y, v.z, v.w};
-        const uint32_t s0 = p0 >> shift;
-        const float inv_a = __ldg(inv + s0), inv_b = __ldg(inv + min(s0 + 1u, 63u));
-#pragma unroll
-        for (uint32_t j = 0; j < 4; j++) {
-            const uint32_t p = p0 + j;
-            if (p < n_blocks) continue;
-            const int32_t q = quantise1(vv[j], ((p >> shift) == s0) ? inv_a : inv_b, kAcRounding);
-            if (q != 0) {
-                const uint32_t run = p - pos;
-                const uint32_t level = (q < 0 ? 0u - (uint32_t)q : (uint32_t)q) - 1u;
-                const Codebook rb = run_book(prev_run), lb = level_book(prev_level);
-                const uint32_t rl = t.run_len(prev_run, run), ll = t.level_len(prev_level, level);
-                if (rl + ll + 1u <= 32u) {
-                    w.put((((cb_bits(rb, run) << ll) | cb_bits(lb, level)) << 1) | (uint64_t)(q < 0), rl + ll + 1u);
-                } else {
-                    w.put_long(cb_bits(rb, run), rl);
-                    w.put_long(cb_bits(lb, level), ll);
-                    w.put((uint64_t)(q < 0), 1);
-                }
-                prev_run = run;
-                prev_level = level;
-                pos = p + 1;
-            }
+    ac_walk(f, n_blocks, inv, [&](const AcWalk &a, uint32_t run, uint32_t level, bool neg) {
+        const Codebook rb = run_book(a.prev_run), lb = level_book(a.prev_level);
+        const uint32_t rl = t.run_len(a.prev_run, run), ll = t.level_len(a.prev_level, level);
+        // Run, level and sign in one field when they fit.
+        if (rl + ll + 1u <= 32u) {
+            w.put((((cb_bits(rb, run) << ll) | cb_bits(lb, level)) << 1) | (uint64_t)neg, rl + ll + 1u);
+        } else {
+            w.put_long(cb_bits(rb, run), rl);
+            w.put_long(cb_bits(lb, level), ll);
+            w.put((uint64_t)neg, 1);
         }
-    }
+    });
     w.finish();
 }
 
@@ -1133,7 +1169,12 @@ cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s)
 
 cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s) {
     if (!e.n_pics) return cudaSuccess;
+    k_share_prep<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
     k_shareout<<<(e.n_pics + kShareWarps - 1) / kShareWarps, 32 * kShareWarps, 0, s>>>(e);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    k_share_final<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);
     return cudaGetLastError();
 }
 

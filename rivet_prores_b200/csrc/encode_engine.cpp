@@ -268,8 +268,12 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     o += 4 * 3 * ns;
     e.final_qi = reinterpret_cast<uint32_t *>(base + o);
     o += 4 * ns;
-    o = (o + 7) & ~(size_t)7;
+    o = (o + 15) & ~(size_t)15;
     e.slice_off = reinterpret_cast<uint64_t *>(base + o);
+    o += 8 * ns;
+    e.share_prep = reinterpret_cast<SharePrep *>(base + o);
+    o += sizeof(SharePrep) * ns;
+    e.share_steps = reinterpret_cast<uint32_t *>(base + o);
     e.out = ws.enc_out.as<uint32_t>();
     e.headers = ws.enc_frame_out.as<uint8_t>();
     e.frame_status = ws.enc_alpha_bits.as<uint32_t>();
@@ -284,7 +288,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
 
 static size_t cost_bytes(const EncodePlan &plan) {
     const size_t ns = plan.n_slices + 1;
-    return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + 64;
+    return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 256;
 }
 
 static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s) {

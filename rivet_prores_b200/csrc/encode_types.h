@@ -72,6 +72,16 @@ struct EncPicState {
 // A window entry that was not costed (the share-out costs it if needed).
 constexpr uint32_t kNotCosted = 0xFFFFFFFFu;
 
+// A slice's share-out inputs: its size at the uniform quantiser, and per
+// window level (bit j of `known` when costed) the smallest D that lets it
+// step there (~0 when the size does not fit) and the size over the base.
+struct SharePrep {
+    uint64_t thr[kWindow];
+    int32_t delta[kWindow];
+    uint32_t base;
+    uint32_t known;
+};
+
 struct EncodeLaunch {
     const uint16_t *in;        // input planes
     const uint16_t *alpha_in;  // input alpha planes
@@ -88,6 +98,8 @@ struct EncodeLaunch {
     uint32_t *final_comp;  // [slice][3]
     uint32_t *final_qi;    // [slice]
     uint64_t *slice_off;   // [slice] byte offset of the slice in its frame
+    SharePrep *share_prep; // [slice]
+    uint32_t *share_steps; // [slice] finer steps taken (top bit: sizes already in final_comp)
     uint32_t *out;         // output buffer (zeroed before packing), big-endian bit order
     const uint8_t *headers;  // frame header templates
     uint32_t *frame_status;  // per frame: 0, or 1 when the frame outgrew its region
