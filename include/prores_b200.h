@@ -218,7 +218,8 @@ int prores_encode_job_create(prores_ctx *ctx, const prores_config *cfg, const pr
                              prores_encode_job **job);
 int prores_encode_job_launch(prores_encode_job *job, void *stream, int use_graph);
 int prores_encode_job_upload(prores_encode_job *job, const prores_frame *in, int n, void *stream);
-/* Waits for `stream`; out[i].data points into job-owned host memory valid
+/* Waits for `stream`; out[i].data points into job-owned pinned host memory
+ * (so it can feed a decode upload without a staging copy), valid
  * until the next fetch or destroy. */
 int prores_encode_job_fetch(prores_encode_job *job, void *stream, prores_buf *out, int *status);
 void prores_encode_job_destroy(prores_encode_job *job);

@@ -99,6 +99,7 @@ __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_
 
 __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
     __shared__ float tmp[kMaxSliceCoefs];  // [comp][y][u][blk]
+    extern __shared__ __align__(16) float scanned[];  // kMaxSliceCoefs: the slice in scanned order
     __shared__ float basis[64];
     __shared__ uint8_t scan[64];
     const EncSliceDesc sd = e.slices[blockIdx.x];
@@ -172,12 +173,12 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
     }
     __syncthreads();
 
-    // Pass 2: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0, written
-    // to the scanned position n * scan[8v + u] + blk of the component.
-    float *gout = e.coef + sd.coef;
+    // Pass 2: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0, put at
+    // the scanned position n * scan[8v + u] + blk of the component.
     for (uint32_t c = 0; c < 3; c++) {
         const uint32_t nb = nbk[c];
         const float *src = tmp + start[c];
+        float *dst = scanned + start[c];
         for (uint32_t t = tid; t < 8u * nb; t += kFdctThreads) {
             const uint32_t blk = t % nb, u = t / nb;
             float col[8];
@@ -188,9 +189,26 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
                 float s = 0.0f;
 #pragma unroll
                 for (int y = 0; y < 8; y++) s = __fadd_rn(s, __fmul_rn(basis[8 * y + v], col[y]));
-                gout[start[c] + nb * scan[8 * v + u] + blk] = s;
+                dst[nb * scan[8 * v + u] + blk] = s;
             }
         }
+    }
+    __syncthreads();
+
+    // The slice out in 16-byte stores, with the largest |F| of each chunk of
+    // 32 coefficients (eight lanes' stores). The slice holds a multiple of
+    // 512 coefficients, so whole warps take part in every shuffle.
+    const uint32_t n4 = (64u * (nbk[0] + 2u * nbk[1])) / 4u;
+    float4 *gout = reinterpret_cast<float4 *>(e.coef + sd.coef);
+    const float4 *sin = reinterpret_cast<const float4 *>(scanned);
+    for (uint32_t i = tid; i < n4; i += kFdctThreads) {
+        const float4 v = sin[i];
+        gout[i] = v;
+        float m = fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
+        if ((i & 7u) == 0) e.coef_max[(sd.coef >> 5) + (i >> 3)] = m;
     }
 }
 
@@ -340,11 +358,12 @@ struct LenTables {
 // The DC part of the bit count (src/encode.rs:383-395): EG5 of the first,
 // then Table 9 by |previous difference|, the sign flipped after a negative
 // one.
-__device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, float inv0) {
+template <class Get>
+__device__ __forceinline__ uint32_t dc_bits_of(Get get, uint32_t n_blocks, float inv0) {
     uint32_t bits = 0;
     int32_t prev_dc = 0, prev_diff = 3;
     for (uint32_t i = 0; i < n_blocks; i++) {
-        const int32_t q = quantise1(__ldg(f + i), inv0, 0.5f);
+        const int32_t q = quantise1(get(i), inv0, 0.5f);
         if (i == 0) {
             bits += cb_len(kFirstDcBook, signed_to_symbol(q));
         } else {
@@ -355,6 +374,10 @@ __device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, f
         prev_dc = q;
     }
     return bits;
+}
+
+__device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, float inv0) {
+    return dc_bits_of([&](uint32_t i) { return __ldg(f + i); }, n_blocks, inv0);
 }
 
 // One AC position of a lane's walk: x = F inv, m = floor(|x| + 0.42)
@@ -379,47 +402,134 @@ __device__ __forceinline__ void ac_position(AcWalk &w, float f, float inv, uint3
     }
 }
 
-// Walks a component's AC positions (n_blocks onwards), four coefficients a
-// load; with two blocks a load spans two scan positions.
+// One component's view of a quantiser table (layout beside kQuantStride):
+// inverse weights and non-zero bounds by scanned position, and the bound of
+// each 32-coefficient chunk of a component of its block count.
+struct CompQuant {
+    const float *inv, *bound, *chunk;
+};
+
+__device__ __forceinline__ CompQuant comp_quant(const float *qb, uint32_t comp, uint32_t n_blocks) {
+    const uint32_t g = comp > 0 ? 1u : 0u;
+    CompQuant c;
+    c.inv = qb + 64u * g;
+    c.bound = qb + 128u + 64u * g;
+    c.chunk = n_blocks >= 32u ? c.bound : qb + 256u + 60u * g + (2u * n_blocks - 4u);
+    return c;
+}
+
+// Whether chunk j holds no coefficient that quantises to a non-zero: its
+// largest |F| is below the least non-zero bound of its positions.
+__device__ __forceinline__ bool chunk_is_zero(const float *cmax, const CompQuant &q, uint32_t j) {
+    return __ldg(cmax + j) < __ldg(q.chunk + j);
+}
+
+// Walks a component's AC positions (n_blocks onwards) in order, position by
+// position, skipping the chunks that quantise to zero; `emit` gets every
+// position's coefficient and inverse weight.
 template <class Emit>
-__device__ __forceinline__ void ac_walk(const float *f, uint32_t n_blocks, const float *inv, Emit emit) {
+__device__ __forceinline__ void ac_walk_dense(const float *f, const float *cmax, uint32_t n_blocks,
+                                              const CompQuant &q, Emit emit) {
+    const uint32_t total = 64u * n_blocks;
+    const uint32_t shift = 31u - __clz(n_blocks);
+    for (uint32_t c0 = n_blocks & ~31u; c0 < total; c0 += 32) {
+        if (chunk_is_zero(cmax, q, c0 >> 5)) continue;
+        if (n_blocks >= 4) {
+            for (uint32_t p0 = max(c0, n_blocks); p0 < c0 + 32u; p0 += 4) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+                const float iv = __ldg(q.inv + (p0 >> shift));
+                emit(v.x, iv, p0);
+                emit(v.y, iv, p0 + 1);
+                emit(v.z, iv, p0 + 2);
+                emit(v.w, iv, p0 + 3);
+            }
+        } else {
+            // Two blocks: positions 0 and 1 are the DCs; p and p + 1 share
+            // scan position p / 2.
+            for (uint32_t p0 = c0; p0 < c0 + 32u; p0 += 4) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+                const float ia = __ldg(q.inv + (p0 >> 1)), ib = __ldg(q.inv + (p0 >> 1) + 1);
+                if (p0 > 0) {
+                    emit(v.x, ia, p0);
+                    emit(v.y, ia, p0 + 1);
+                }
+                emit(v.z, ib, p0 + 2);
+                emit(v.w, ib, p0 + 3);
+            }
+        }
+    }
+}
+
+// The same walk over candidates only: a chunk's candidate mask takes one
+// compare per coefficient against the non-zero bound of its position (so
+// it holds every non-zero, and each candidate is re-quantised exactly),
+// and the lane then visits the candidates alone. Suited to heavy per-code
+// work (the writer), where a position-by-position walk would make every
+// lane wait out every other lane's codes.
+template <class Emit>
+__device__ __forceinline__ void ac_walk_sparse(const float *f, const float *cmax, uint32_t n_blocks,
+                                               const CompQuant &q, Emit emit) {
     const uint32_t total = 64u * n_blocks;
     const uint32_t shift = 31u - __clz(n_blocks);
     AcWalk w;
     w.pos = n_blocks;
-    if (n_blocks >= 4) {
-        for (uint32_t p0 = n_blocks; p0 < total; p0 += 4) {
-            const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
-            const float iv = __ldg(inv + (p0 >> shift));
-            ac_position(w, v.x, iv, p0, emit);
-            ac_position(w, v.y, iv, p0 + 1, emit);
-            ac_position(w, v.z, iv, p0 + 2, emit);
-            ac_position(w, v.w, iv, p0 + 3, emit);
+    for (uint32_t c0 = n_blocks & ~31u; c0 < total; c0 += 32) {
+        if (chunk_is_zero(cmax, q, c0 >> 5)) continue;
+        uint32_t mask = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < 8; i++) {
+            const uint32_t e0 = c0 + 4u * i;
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(f + e0));
+            // With two blocks a load spans scan positions e0 / 2 and e0 / 2 + 1.
+            const float ta = __ldg(q.bound + (e0 >> shift)), tb = __ldg(q.bound + ((e0 + 3u) >> shift));
+            const uint32_t nib = (fabsf(v.x) >= ta ? 1u : 0u) | (fabsf(v.y) >= ta ? 2u : 0u) |
+                                 (fabsf(v.z) >= tb ? 4u : 0u) | (fabsf(v.w) >= tb ? 8u : 0u);
+            mask |= nib << (4u * i);
         }
-    } else {
-        // Two blocks: positions 0 and 1 are the DCs; p and p + 1 share scan
-        // position p / 2.
-        for (uint32_t p0 = 0; p0 < total; p0 += 4) {
-            const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
-            const float ia = __ldg(inv + (p0 >> 1)), ib = __ldg(inv + (p0 >> 1) + 1);
-            if (p0 > 0) {
-                ac_position(w, v.x, ia, p0, emit);
-                ac_position(w, v.y, ia, p0 + 1, emit);
-            }
-            ac_position(w, v.z, ib, p0 + 2, emit);
-            ac_position(w, v.w, ib, p0 + 3, emit);
+        if (c0 == 0) mask &= ~0u << n_blocks;  // the DCs
+        while (mask) {
+            const uint32_t p = c0 + (uint32_t)__ffs(mask) - 1u;
+            mask &= mask - 1u;
+            ac_position(w, __ldg(f + p), __ldg(q.inv + (p >> shift)), p, emit);
         }
+    }
+}
+
+// The AC part of a lane's bit count at one position: the position is
+// quantised and its code length (run by the previous run's context, level
+// by the previous level's, a sign bit) taken from the length tables
+// whether or not it is a non-zero, and kept only if it is. Lanes that count
+// different components so stay in step, with no branch per position; only
+// a run or level past the tables (32 and above) takes a branch.
+struct AcCount {
+    uint32_t bits = 0, pos = 0, run_ctx = 4, level_ctx = 1;
+};
+
+__device__ __forceinline__ void count_position(AcCount &c, float f, float inv, uint32_t p, const LenTables &t) {
+    const float x = __fmul_rn(f, inv);
+    const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
+    const bool nz = m >= 1.0f;
+    const uint32_t run = p - c.pos;
+    const uint32_t level = (uint32_t)__float2int_rz(m) - 1u;
+    uint32_t add = (uint32_t)t.run[c.run_ctx][min(run, 31u)] + (uint32_t)t.level[c.level_ctx][min(level, 31u)] + 1u;
+    if (nz && (run | level) >= 32u)
+        add = cb_len(run_book(c.run_ctx), run) + cb_len(level_book(c.level_ctx), level) + 1u;
+    if (nz) {
+        c.bits += add;
+        c.run_ctx = min(run, 15u);
+        c.level_ctx = min(level, 8u);
+        c.pos = p + 1u;
     }
 }
 
 // Bits of one quantised component (src/encode.rs:398-409), one lane: the
 // crate's own walk over the scanned positions.
-__device__ uint32_t lane_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
-    uint32_t bits = dc_bits(f, n_blocks, __ldg(inv));
-    ac_walk(f, n_blocks, inv, [&](const AcWalk &w, uint32_t run, uint32_t level, bool) {
-        bits += t.run_len(w.prev_run, run) + t.level_len(w.prev_level, level) + 1u;
-    });
-    return bits;
+__device__ uint32_t lane_component_bits(const float *f, const float *cmax, uint32_t n_blocks, const CompQuant &q,
+                                        const LenTables &t) {
+    AcCount c;
+    c.pos = n_blocks;
+    ac_walk_dense(f, cmax, n_blocks, q, [&](float v, float inv, uint32_t p) { count_position(c, v, inv, p, t); });
+    return dc_bits(f, n_blocks, __ldg(q.inv)) + c.bits;
 }
 
 // The same count with a whole warp on one component, for when latency
@@ -427,7 +537,9 @@ __device__ uint32_t lane_component_bits(const float *f, uint32_t n_blocks, const
 // needs): lane l takes scanned positions 32 k + l; a non-zero's run and its
 // contexts (the previous non-zero's run and level symbol) come from the
 // lanes below it or from what the last step carried.
-__device__ uint32_t warp_component_bits(const float *f, uint32_t n_blocks, const float *inv, const LenTables &t) {
+__device__ uint32_t warp_component_bits(const float *f, const float *cmax, uint32_t n_blocks, const CompQuant &cq,
+                                        const LenTables &t) {
+    const float *inv = cq.inv;
     const int lane = threadIdx.x & 31;
     const uint32_t total = 64u * n_blocks;
     const uint32_t shift = 31u - __clz(n_blocks);
@@ -435,6 +547,8 @@ __device__ uint32_t warp_component_bits(const float *f, uint32_t n_blocks, const
     int32_t carry_pos = (int32_t)n_blocks - 1;
     uint32_t carry_run = 4, carry_level = 1;
     for (uint32_t base = 0; base < total; base += 32) {
+        // Past the DCs a chunk that quantises to zero changes nothing.
+        if (base > 0 && chunk_is_zero(cmax, cq, base >> 5)) continue;
         const uint32_t p = base + lane;
         const uint32_t sidx = p >> shift;
         const int32_t q = quantise1(__ldg(f + p), __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
@@ -473,9 +587,9 @@ __device__ uint32_t warp_component_bits(const float *f, uint32_t n_blocks, const
     return bits;
 }
 
-__device__ __forceinline__ const float *quant_table(const EncodeLaunch &e, const EncPicDesc &pd, uint32_t qi,
-                                                    uint32_t comp) {
-    return e.quant + ((uint64_t)pd.quant * 225u + qi) * 128u + (comp > 0 ? 64u : 0u);
+// The quantiser table of quantization_index qi (layout beside kQuantStride).
+__device__ __forceinline__ const float *quant_base(const EncodeLaunch &e, const EncPicDesc &pd, uint32_t qi) {
+    return e.quant + ((uint64_t)pd.quant * 225u + qi) * kQuantStride;
 }
 
 __device__ __forceinline__ void comp_layout(const EncFrameDesc &fd, uint32_t mbs, uint32_t comp, uint32_t &n_blocks,
@@ -491,7 +605,8 @@ __device__ __forceinline__ uint32_t component_bytes(const EncodeLaunch &e, const
                                                     const LenTables &t) {
     uint32_t nb, off;
     comp_layout(fd, sd.mbs, comp, nb, off);
-    const uint32_t bits = lane_component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp), t);
+    const CompQuant q = comp_quant(quant_base(e, pd, qi), comp, nb);
+    const uint32_t bits = lane_component_bits(e.coef + sd.coef + off, e.coef_max + ((sd.coef + off) >> 5), nb, q, t);
     return (bits + 7u) / 8u;
 }
 
@@ -501,7 +616,8 @@ __device__ __forceinline__ uint32_t warp_component_bytes(const EncodeLaunch &e, 
                                                          uint32_t qi, const LenTables &t) {
     uint32_t nb, off;
     comp_layout(fd, sd.mbs, comp, nb, off);
-    const uint32_t bits = warp_component_bits(e.coef + sd.coef + off, nb, quant_table(e, pd, qi, comp), t);
+    const CompQuant q = comp_quant(quant_base(e, pd, qi), comp, nb);
+    const uint32_t bits = warp_component_bits(e.coef + sd.coef + off, e.coef_max + ((sd.coef + off) >> 5), nb, q, t);
     return (bits + 7u) / 8u;
 }
 
@@ -564,53 +680,76 @@ __device__ __forceinline__ const uint32_t *level_comp(const EncodeLaunch &e, con
     return e.win_comp + ((uint64_t)j * e.n_slices + s) * 3u;
 }
 
-// Window level j: the first for every slice; the next ones for the slices
+// The slices whose window level is costed, as a list: level 0 takes every
+// slice of a picture that has finer quantisers to share out (unless the
+// failed probe at uniform - 1 sized them already); a later level the slices
 // whose size at the level before fits and is within the most their share
-// can come to (the crate's prefetch rule, src/encode.rs:741-767).
+// can come to (the crate's prefetch rule, src/encode.rs:741-767). The list
+// order is the atomics' and steers nothing but speed.
+__global__ void __launch_bounds__(kCostThreads) k_window_select(EncodeLaunch e, int level) {
+    const uint32_t s = blockIdx.x * kCostThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool take = false;
+    if (s < e.n_slices) {
+        const EncSliceDesc sd = e.slices[s];
+        const EncPicState st = e.state[sd.pic];
+        const int32_t qi = st.uniform - 1 - level;
+        if (st.fits_at_all && st.uniform > 1 && qi >= 1 && !(level == 0 && st.lo_probe >= 0)) {
+            take = true;
+            if (level > 0) {
+                const EncPicDesc &pd = e.pics[sd.pic];
+                const uint32_t *prev = level_comp(e, st, (uint32_t)level - 1u, s);
+                take = prev[0] != kNotCosted;
+                if (take) {
+                    const uint32_t alpha = e.alpha_bytes[s];
+                    const uint32_t pc[3] = {prev[0], prev[1], prev[2]};
+                    bool fits, f2;
+                    const uint64_t n = slice_total(pd.header_bytes, pc, alpha, fits);
+                    const uint32_t *u = e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u;
+                    const uint32_t uc[3] = {u[0], u[1], u[2]};
+                    const uint64_t used = slice_total(pd.header_bytes, uc, alpha, f2);
+                    const uint64_t slack = st.budget - st.hi_total;
+                    const uint64_t most = used + slack * sd.mbs / mbs_from(pd, sd);
+                    take = fits && n <= most;
+                }
+                if (!take) e.win_comp[((uint64_t)level * e.n_slices + s) * 3u] = kNotCosted;
+            }
+        }
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, take);
+    if (m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t at = 0;
+        if (lane == leader) at = atomicAdd(e.win_count + level, (uint32_t)__popc(m));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (take) e.win_list[at + __popc(m & ((1u << lane) - 1u))] = s;
+    }
+}
+
+// Costs the listed slices at window level `level` (quantiser uniform - 1 -
+// level): a lane per (component, slice), component-major, or a warp each.
 template <bool kWarp>
 __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, int level) {
     __shared__ LenTables t;
+    const uint32_t n = e.win_count[level];
+    if (blockIdx.x * (kWarp ? kCostThreads / 32 : kCostThreads) >= 3u * n) return;  // the whole block
     t.fill();
     __syncthreads();
     const uint32_t item = kWarp ? blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5)
                                 : blockIdx.x * kCostThreads + threadIdx.x;
-    if (item >= 3u * e.n_slices) return;
-    const uint32_t comp = kWarp ? item % 3u : item / e.n_slices;
-    const uint32_t s = kWarp ? item / 3u : item - comp * e.n_slices;
+    if (item >= 3u * n) return;
+    const uint32_t comp = kWarp ? item % 3u : item / n;
+    const uint32_t s = e.win_list[kWarp ? item / 3u : item - comp * n];
     const EncSliceDesc sd = e.slices[s];
-    const EncPicState st = e.state[sd.pic];
-    if (!(st.fits_at_all && st.uniform > 1)) return;
-    const int32_t qi = st.uniform - 1 - level;
-    if (qi < 1) return;
-    if (level == 0 && st.lo_probe >= 0) return;  // probed already
+    const uint32_t qi = (uint32_t)(e.state[sd.pic].uniform - 1 - level);
     const EncPicDesc &pd = e.pics[sd.pic];
     const EncFrameDesc &fd = e.frames[pd.frame];
     uint32_t *out = e.win_comp + ((uint64_t)level * e.n_slices + s) * 3u;
-    if (level > 0) {
-        const uint32_t *prev = level_comp(e, st, (uint32_t)level - 1u, s);
-        bool wanted = prev[0] != kNotCosted;
-        if (wanted) {
-            const uint32_t alpha = e.alpha_bytes[s];
-            const uint32_t pc[3] = {prev[0], prev[1], prev[2]};
-            bool fits, f2;
-            const uint64_t n = slice_total(pd.header_bytes, pc, alpha, fits);
-            const uint32_t *u = e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u;
-            const uint32_t uc[3] = {u[0], u[1], u[2]};
-            const uint64_t used = slice_total(pd.header_bytes, uc, alpha, f2);
-            const uint64_t slack = st.budget - st.hi_total;
-            const uint64_t most = used + slack * sd.mbs / mbs_from(pd, sd);
-            wanted = fits && n <= most;
-        }
-        if (!wanted) {
-            if (comp == 0 && (!kWarp || (threadIdx.x & 31) == 0)) out[0] = kNotCosted;
-            return;
-        }
-    }
     if (kWarp) {
-        const uint32_t bytes = warp_component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+        const uint32_t bytes = warp_component_bytes(e, sd, pd, fd, comp, qi, t);
         if ((threadIdx.x & 31) == 0) out[comp] = bytes;
     } else {
-        out[comp] = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+        out[comp] = component_bytes(e, sd, pd, fd, comp, qi, t);
     }
 }
 
@@ -649,6 +788,8 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_init(EncodeLaunch e) {
         st.fits_at_all = 0;
         st.uniform = 224;
         e.state[blockIdx.x] = st;
+        if (blockIdx.x == 0)
+            for (int j = 0; j < kWindow; j++) e.win_count[j] = 0;
     }
 }
 
@@ -1016,9 +1157,9 @@ struct BitOut {
 };
 
 // One quantised component's codes (src/encode.rs:413-437), one lane.
-__device__ void lane_component_write(BitOut &w, const float *f, uint32_t n_blocks, const float *inv,
-                                     const LenTables &t) {
-    const float inv0 = __ldg(inv);
+__device__ void lane_component_write(BitOut &w, const float *f, const float *cmax, uint32_t n_blocks,
+                                     const CompQuant &q, const LenTables &t) {
+    const float inv0 = __ldg(q.inv);
     int32_t prev_dc = 0, prev_diff = 3;
     for (uint32_t i = 0; i < n_blocks; i++) {
         const int32_t q = quantise1(__ldg(f + i), inv0, 0.5f);
@@ -1036,7 +1177,7 @@ __device__ void lane_component_write(BitOut &w, const float *f, uint32_t n_block
         w.put_long(cb_bits(cb, sym), cb_len(cb, sym));
         prev_dc = q;
     }
-    ac_walk(f, n_blocks, inv, [&](const AcWalk &a, uint32_t run, uint32_t level, bool neg) {
+    ac_walk_sparse(f, cmax, n_blocks, q, [&](const AcWalk &a, uint32_t run, uint32_t level, bool neg) {
         const Codebook rb = run_book(a.prev_run), lb = level_book(a.prev_level);
         const uint32_t rl = t.run_len(a.prev_run, run), ll = t.level_len(a.prev_level, level);
         // Run, level and sign in one field when they fit.
@@ -1070,7 +1211,8 @@ __global__ void __launch_bounds__(kCostThreads) k_pack(EncodeLaunch e) {
     comp_layout(fd, sd.mbs, comp, nb, off);
     BitOut w;
     w.init(e.out, at);
-    lane_component_write(w, e.coef + sd.coef + off, nb, quant_table(e, pd, e.final_qi[s], comp), t);
+    lane_component_write(w, e.coef + sd.coef + off, e.coef_max + ((sd.coef + off) >> 5), nb,
+                         comp_quant(quant_base(e, pd, e.final_qi[s]), comp, nb), t);
 }
 
 // Slice headers and table entries, one thread per slice; alpha codes, one
@@ -1117,7 +1259,7 @@ __global__ void __launch_bounds__(32 * kAlphaWarps) k_pack_alpha(EncodeLaunch e)
 
 cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
-    k_fdct<<<e.n_slices, kFdctThreads, 0, s>>>(e);
+    k_fdct<<<e.n_slices, kFdctThreads, 4 * kMaxSliceCoefs, s>>>(e);
     return cudaGetLastError();
 }
 
@@ -1158,9 +1300,11 @@ cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s) {
 cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
     const uint32_t items = 3u * e.n_slices;
-    // Level 0 covers every slice; the later levels only the few candidates,
-    // so their latency is what counts.
-    if (level == 0 && lane_mode(e))
+    k_window_select<<<(e.n_slices + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, level);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    // The grid covers every slice; blocks past the list's end return.
+    if (lane_mode(e))
         k_cost_window<false><<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, level);
     else
         k_cost_window<true><<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, level);
@@ -1199,6 +1343,10 @@ cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
 }
 
 cudaError_t configure_encode_kernels() {
+    // 24 KB of static and 24 KB of dynamic shared memory pass the 48 KB that
+    // needs no opt-in.
+    cudaError_t err = cudaFuncSetAttribute(k_fdct, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kMaxSliceCoefs);
+    if (err != cudaSuccess) return err;
     uint8_t sc[2][64];
     for (int i = 0; i < 64; i++) {
         sc[0][i] = kProgressiveScan[i];

@@ -9,6 +9,7 @@
 // a frame that outgrows its region (possible only when even quantiser 224
 // misses the target) is laid out again in a larger one.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -100,8 +101,24 @@ static Status validate(const prores_config &cfg, const prores_frame &f, int *alp
     return Status();
 }
 
-// inv[scan[k]] = 8 / (W[k] qScale) in single precision, for luma and chroma
-// and every quantization_index (src/encode.rs:303-329).
+// A lower bound on the |F| that quantise to a non-zero AC level at inverse
+// weight inv. A level is non-zero when fl(fl(|F| inv) + 0.42f) >= 1, which
+// needs the exact sum fl(|F| inv) + 0.42f to reach 1 - 2^-25 (the midpoint
+// below 1), and so |F| inv >= (1 - 2^-25 - 0.42f)(1 - 2^-24). The bound takes
+// a margin of 2^-22 and is rounded down, so every non-zero lies at or above
+// it; the kernels re-quantise each candidate exactly.
+static float nonzero_bound(float inv) {
+    const double y0 = 1.0 - std::ldexp(1.0, -25) - (double)0.42f;
+    const double t = y0 * (1.0 - std::ldexp(1.0, -22)) / (double)inv;
+    float b = (float)t;
+    if ((double)b > t) b = std::nextafter(b, 0.0f);
+    return b;
+}
+
+// Per quantization_index, kQuantStride floats (the layout is given beside
+// kQuantStride): inv[scan[k]] = 8 / (W[k] qScale) in single precision for
+// luma and chroma (src/encode.rs:303-329), the non-zero bound of each, and
+// the least bound over each chunk of 32 scanned coefficients.
 static uint32_t add_quant(EncodePlan &plan, const FrameHeader &h) {
     uint8_t key[129];
     h.luma_weights(key);
@@ -112,13 +129,25 @@ static uint32_t add_quant(EncodePlan &plan, const FrameHeader &h) {
     plan.quant_keys.insert(plan.quant_keys.end(), key, key + 129);
     const uint8_t *scan = h.interlace ? kInterlacedScan : kProgressiveScan;
     const size_t base = plan.quant.size();
-    plan.quant.resize(base + 225 * 128);
+    plan.quant.resize(base + 225 * kQuantStride);
     for (uint32_t qi = 0; qi <= 224; qi++) {
         const uint32_t q = qscale(qi < 1 ? 1 : qi);
-        float *t = &plan.quant[base + qi * 128];
+        float *t = &plan.quant[base + qi * kQuantStride];
         for (int k = 0; k < 64; k++) {
             t[scan[k]] = 8.0f / (float)((uint32_t)key[k] * q);
             t[64 + scan[k]] = 8.0f / (float)((uint32_t)key[64 + k] * q);
+        }
+        for (int k = 0; k < 128; k++) t[128 + k] = nonzero_bound(t[k]);
+        for (uint32_t g = 0; g < 2; g++) {
+            const float *bound = t + 128 + 64 * g;
+            for (uint32_t n = 2; n <= 16; n *= 2) {
+                float *chunk = t + 256 + 60 * g + (2 * n - 4);
+                for (uint32_t j = 0; j < 2 * n; j++) {
+                    float m = bound[32 * j / n];
+                    for (uint32_t k = 32 * j / n; k < 32 * (j + 1) / n; k++) m = std::min(m, bound[k]);
+                    chunk[j] = m;
+                }
+            }
         }
     }
     return (uint32_t)(plan.quant_keys.size() / 129 - 1);
@@ -254,6 +283,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     e.slices = ws.slices.as<EncSliceDesc>();
     e.state = ws.enc_pic_state.as<EncPicState>();
     e.coef = ws.enc_coef.as<float>();
+    e.coef_max = e.coef + plan.coef_total + 64;
     e.quant = ws.weights.as<float>();
     e.basis = ctx.tables.basis;
     // The per-slice tables share one allocation.
@@ -274,6 +304,10 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     e.share_prep = reinterpret_cast<SharePrep *>(base + o);
     o += sizeof(SharePrep) * ns;
     e.share_steps = reinterpret_cast<uint32_t *>(base + o);
+    o += 4 * ns;
+    e.win_list = reinterpret_cast<uint32_t *>(base + o);
+    o += 4 * ns;
+    e.win_count = reinterpret_cast<uint32_t *>(base + o);
     e.out = ws.enc_out.as<uint32_t>();
     e.headers = ws.enc_frame_out.as<uint8_t>();
     e.frame_status = ws.enc_alpha_bits.as<uint32_t>();
@@ -288,7 +322,8 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
 
 static size_t cost_bytes(const EncodePlan &plan) {
     const size_t ns = plan.n_slices + 1;
-    return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 256;
+    return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 4 * ns +
+           4 * kWindow + 256;
 }
 
 static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s) {
@@ -330,7 +365,8 @@ Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores
         PR_CUDA(ws.pics.reserve(sizeof(EncPicDesc) * (plan.pdesc.size() + 1)), "cudaMalloc");
         PR_CUDA(ws.slices.reserve(sizeof(EncSliceDesc) * (plan.n_slices + 1)), "cudaMalloc");
         PR_CUDA(ws.enc_pic_state.reserve(sizeof(EncPicState) * (plan.pdesc.size() + 1)), "cudaMalloc");
-        PR_CUDA(ws.enc_coef.reserve(4 * (plan.coef_total + 64)), "cudaMalloc coefficients");
+        // The coefficients, then (64 floats on) one chunk maximum per 32.
+    PR_CUDA(ws.enc_coef.reserve(4 * (plan.coef_total + plan.coef_total / 32 + 128)), "cudaMalloc coefficients");
         PR_CUDA(ws.weights.reserve(4 * (plan.quant.size() + 64)), "cudaMalloc");
         PR_CUDA(ws.enc_cost.reserve(cost_bytes(plan)), "cudaMalloc");
         PR_CUDA(ws.enc_out.reserve(plan.out_total + 64), "cudaMalloc output");
@@ -395,8 +431,8 @@ Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_
     return enqueue_tail(ctx, ws, plan, s, kt);
 }
 
-Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s,
-                    std::vector<std::vector<uint8_t>> &out, int *status, Status *first_err) {
+Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, std::vector<prores_buf> &out,
+                    int *status, Status *first_err) {
     const size_t nf = plan.fdesc.size();
     for (int attempt = 0; attempt < 2; attempt++) {
         if (nf) {
@@ -441,7 +477,7 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
         pos += plan.frame_size[f];
     }
     PR_CUDA(cudaStreamSynchronize(s), "encode");
-    out.assign(plan.frames.size(), {});
+    out.assign(plan.frames.size(), prores_buf{nullptr, 0});
     pos = 0;
     std::vector<Status> errs(plan.frames.size());
     for (size_t i = 0; i < plan.frames.size(); i++) {
@@ -453,8 +489,8 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
             continue;
         }
         const size_t n = plan.frame_size[ef.desc];
-        const uint8_t *src = static_cast<uint8_t *>(ws.host_stage.p) + pos;
-        out[i].assign(src, src + n);
+        out[i].data = static_cast<uint8_t *>(ws.host_stage.p) + pos;
+        out[i].len = n;
         pos += n;
     }
     set_batch_errors(errs);
@@ -492,7 +528,7 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
     cudaStream_t s = ws->stream;
     st = upload_encode(ctx->impl, *ws, *plan, in, s, true);
     if (!st) st = enqueue_encode(ctx->impl, *ws, *plan, s, nullptr);
-    std::vector<std::vector<uint8_t>> packets;
+    std::vector<prores_buf> packets;
     Status first;
     if (!st) st = fetch_encode(ctx->impl, *ws, *plan, s, packets, status, &first);
     if (st) {
@@ -500,17 +536,26 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
         ctx->impl.release(std::move(ws));
         return efail(st);
     }
-    ctx->impl.release(std::move(ws));
+    // The packets lie in the workspace's staging buffer: copied out before
+    // the workspace goes back to the pool.
     for (int i = 0; i < n; i++) {
         out[i].data = nullptr;
         out[i].len = 0;
-        if (status[i] != PRORES_OK) continue;
-        uint8_t *p = static_cast<uint8_t *>(malloc(packets[i].size() ? packets[i].size() : 1));
-        if (!p) return efail(make_status(PRORES_DEVICE, "host allocation failed"));
-        memcpy(p, packets[i].data(), packets[i].size());
-        out[i].data = p;
-        out[i].len = packets[i].size();
     }
+    for (int i = 0; i < n; i++) {
+        if (status[i] != PRORES_OK) continue;
+        uint8_t *p = static_cast<uint8_t *>(malloc(packets[i].len ? packets[i].len : 1));
+        if (!p) {
+            for (int j = 0; j < i; j++) free(const_cast<uint8_t *>(out[j].data));
+            for (int j = 0; j < i; j++) out[j] = prores_buf{nullptr, 0};
+            ctx->impl.release(std::move(ws));
+            return efail(make_status(PRORES_DEVICE, "host allocation failed"));
+        }
+        memcpy(p, packets[i].data, packets[i].len);
+        out[i].data = p;
+        out[i].len = packets[i].len;
+    }
+    ctx->impl.release(std::move(ws));
     if (first) set_last_error(first);
     return PRORES_OK;
 }
@@ -598,10 +643,7 @@ int prores_encode_job_fetch(prores_encode_job *job, void *stream, prores_buf *ou
     Status first;
     Status st = fetch_encode(job->ctx->impl, *job->ws, *job->plan, s, job->packets, status, &first);
     if (st) return efail(st);
-    for (size_t i = 0; i < job->packets.size(); i++) {
-        out[i].data = job->packets[i].data();
-        out[i].len = job->packets[i].size();
-    }
+    for (size_t i = 0; i < job->packets.size(); i++) out[i] = job->packets[i];
     if (first) set_last_error(first);
     return PRORES_OK;
 }

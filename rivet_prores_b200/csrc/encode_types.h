@@ -82,6 +82,15 @@ struct SharePrep {
     uint32_t known;
 };
 
+// Per quantiser set and quantization_index, kQuantStride floats:
+//   [0, 128)    8 / (W qScale) at the scanned positions, luma then chroma;
+//   [128, 256)  the least |F| that can quantise to a non-zero AC level at each;
+//   [256, 376)  per component group (luma, chroma: 60 each) the least of
+//               those bounds over each 32-coefficient chunk of a component
+//               of n blocks, n = 2, 4, 8, 16 (2n chunks each, at 2n - 4).
+// For n = 32 a chunk is one scanned position, whose bound is in [128, 256).
+constexpr uint32_t kQuantStride = 384;
+
 struct EncodeLaunch {
     const uint16_t *in;        // input planes
     const uint16_t *alpha_in;  // input alpha planes
@@ -90,11 +99,14 @@ struct EncodeLaunch {
     const EncSliceDesc *slices;
     EncPicState *state;
     float *coef;           // transformed slices, scanned order
-    const float *quant;    // [set][225 qi][2][64] 8 / (W qScale) at scanned positions
+    float *coef_max;       // [coef / 32] the largest |F| of each 32 scanned coefficients (a chunk)
+    const float *quant;    // [set][225 qi][kQuantStride], see quant_base
     const float *basis;    // T[x][u]
     uint32_t *alpha_bytes; // per slice
     uint32_t *probe_comp;  // [kProbeSteps][slice][3] component bytes
     uint32_t *win_comp;    // [kWindow][slice][3]
+    uint32_t *win_list;    // [slice] the slices costed at the current window level
+    uint32_t *win_count;   // [kWindow] list lengths
     uint32_t *final_comp;  // [slice][3]
     uint32_t *final_qi;    // [slice]
     uint64_t *slice_off;   // [slice] byte offset of the slice in its frame

@@ -113,8 +113,10 @@ Status plan_encode(const prores_config *cfg, const prores_frame *in, int n, Enco
 Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores_frame *in, cudaStream_t s,
                      bool descriptors);
 Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, KernelTimes *kt);
-Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s,
-                    std::vector<std::vector<uint8_t>> &out, int *status, Status *first_err);
+// Waits for the encode and stages the packets in the workspace's pinned
+// buffer; out[i] points into it until the workspace's next fetch.
+Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, std::vector<prores_buf> &out,
+                    int *status, Status *first_err);
 
 void set_last_error(const Status &s);
 // Per-frame messages of the last batch call on this thread.
@@ -139,6 +141,6 @@ struct prores_encode_job {
     prores_ctx *ctx = nullptr;
     std::unique_ptr<prores::Workspace> ws;
     prores::EncodePlanPtr plan;
-    std::vector<std::vector<uint8_t>> packets;
+    std::vector<prores_buf> packets;  // into the workspace's pinned staging buffer
     prores::KernelTimes kt;
 };
