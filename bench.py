@@ -48,7 +48,9 @@ def parse_args():
     ap.add_argument("--unique", type=int, default=4, help="distinct synthetic pictures in a batch")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-chunks", type=int, default=4, help="streams the end-to-end batch is split over")
+    ap.add_argument("--e2e-chunks", type=int, default=0,
+                    help="parts the end-to-end batch is split over (0: the tuned staging depth)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the cached or default launch shapes")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=4.0, help="0 skips the serving run")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean requests/s (Poisson)")
@@ -193,6 +195,19 @@ def run_b200(args):
     cfg = P.Config(P.Profile.Hq)
     stream = torch.cuda.Stream()
 
+    # Launch shapes: tuned on this GPU before anything is timed (none of them
+    # changes an output).
+    tuning_note = "cached or default"
+    if not args.no_tune:
+        from rivet_prores_b200 import autotune
+
+        autotune.tune(device=local, quick=True, store=False, frames=frames[:8], stage_frames=frames,
+                      depths=[2, 4, 8, 16])
+        tuning_note = "tuned in this run (rivet_prores_b200.autotune, quick search)"
+    from dataclasses import asdict
+
+    tuning = asdict(P.context(local).tuning)
+
     # Resident jobs: the encoder's packets of this batch feed the decoder.
     enc = P.EncodeJob(frames, cfg, device=local)
     enc.launch(stream)
@@ -299,87 +314,30 @@ def run_b200(args):
     for j in penc1 + pdec1:
         j.close()
 
-    # End to end through the C ABI with host buffers: each step copies the
-    # frames in from pinned memory, encodes, reads the packets back, copies
-    # them in, decodes and reads the planes back. The batch goes through in
-    # chunks, each on its own stream and host thread, so that one chunk's
-    # copies overlap another's kernels and both copy directions run at once.
+    # End to end through the C ABI with host buffers (stream.RoundTripPipeline):
+    # each step copies the frames in from pinned memory, encodes, reads the
+    # packets back, copies them in, decodes and reads the planes back, the
+    # batch split into parts on their own streams and host threads.
     e2e = None
     if not args.no_e2e:
-        import concurrent.futures as cf
+        from rivet_prores_b200.stream import RoundTripPipeline, time_round_trip
 
-        n_samples = frames[0].data.size
-        host = torch.empty((B, n_samples), dtype=torch.uint16, pin_memory=True).numpy()
-        out_host = torch.empty((B, n_samples), dtype=torch.uint16, pin_memory=True).numpy()
-        chunks = max(1, min(args.e2e_chunks, B))
-        bounds = [(c * B // chunks, (c + 1) * B // chunks) for c in range(chunks)]
-        lanes = []
-        for lo, hi in bounds:
-            hframes = []
-            for i in range(lo, hi):
-                host[i] = frames[i].data
-                f = frames[i]
-                hframes.append(P.Frame(f.width, f.height, f.bit_depth, f.chroma, f.interlace, f.metadata, host[i],
-                                       f.planes, None))
-            cenc = P.EncodeJob(hframes, cfg, device=local)
-            cdec = P.DecodeJob(packets[lo:hi], device=local)
-            lanes.append({"enc": cenc, "dec": cdec, "frames": hframes, "stream": torch.cuda.Stream(),
-                          "arrays": [(out_host[i], None) for i in range(lo, hi)]})
-
-        def lane_step(lane):
-            st = lane["stream"]
-            lane["enc"].upload(lane["frames"], st)
-            lane["enc"].launch(st, graph=True)
-            pk = lane["enc"].fetch(st, copy=False)
-            lane["dec"].upload([np.frombuffer(p, dtype=np.uint8) for p in pk], st)
-            lane["dec"].launch(st, graph=True)
-            res = lane["dec"].fetch(st, lane["arrays"])
-            lane["end"].record(st)
-            return pk, res
-
-        pool = cf.ThreadPoolExecutor(max_workers=chunks)
-        main = torch.cuda.Stream()
-
-        def e2e_step():
-            start = torch.cuda.Event(enable_timing=True)
-            start.record(main)
-            for lane in lanes:
-                lane["stream"].wait_event(start)
-                lane["end"] = torch.cuda.Event(enable_timing=True)
-            outs = list(pool.map(lane_step, lanes))
-            for lane in lanes:
-                main.wait_event(lane["end"])
-            end = torch.cuda.Event(enable_timing=True)
-            end.record(main)
-            return start, end, outs
-
-        for _ in range(2):
-            e2e_step()
-        main.synchronize()
+        depth = args.e2e_chunks or P.context(local).tuning.staging_depth
+        pipe = RoundTripPipeline(frames, cfg, depth, device=local)
         e2e_steps = max(2, args.steps // 2)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        marks = [e2e_step() for _ in range(e2e_steps)]
-        main.synchronize()
-        t = marks[0][0].elapsed_time(marks[-1][1])
-        outs = marks[-1][2]
-        pk = [p for o in outs for p in o[0]]
-        res = [r for o in outs for r in o[1]]
-        h2d = sum(2 * f.data.size for f in frames) + sum(len(p) for p in pk)
-        d2h = sum(len(p) for p in pk) + sum(2 * out_host[i].size for i in range(B))
+        t = time_round_trip(pipe, e2e_steps, warmup=2) * e2e_steps
+        h2d, d2h = pipe.bytes_per_step()
         t = max_over_ranks([t], dist, "cuda")[0]
         e2e = {"value": round(B * e2e_steps * world / (t / 1000.0), 3), "unit": "frames/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-               "path": f"prores_{{encode,decode}}_job_{{upload,launch,fetch}}, pinned host buffers, "
-                       f"{chunks} chunks on their own streams"}
-        for i, r in enumerate(res):
-            assert np.array_equal(r.data, out_host[i])
-        assert np.array_equal(out_host[0], dec.fetch(stream)[0].data)
-        pool.shutdown()
-        for lane in lanes:
-            lane["enc"].close()
-            lane["dec"].close()
+               "path": f"stream.RoundTripPipeline: prores_{{encode,decode}}_job_{{upload,launch,fetch}}, pinned host "
+                       f"buffers, {len(pipe.parts)} parts on their own streams"}
+        assert [bytes(p) for p in pipe.packets] == packets
+        assert np.array_equal(pipe.planes[0], dec.fetch(stream)[0].data)
+        pipe.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -409,7 +367,8 @@ def run_b200(args):
                    "chroma": "4:2:2", "bit_depth": 10, "profile": "HQ (apch)", "target_frame_bytes": 3_643_238,
                    "step": "encode B frames, then decode their packets; one graph launch each, resident buffers",
                    "l2": "inputs larger than L2 (B x 33 MB of planes per step)",
-                   "parallelism": f"{world} rank(s), frames sharded by rank, no collective"},
+                   "parallelism": f"{world} rank(s), frames sharded by rank, no collective",
+                   "tuning": tuning, "tuning_source": tuning_note},
         "bit_exact": exact,
         "decode_fps": round(dec_fps, 3), "encode_fps": round(enc_fps, 3),
         "plain": {"value": round(plain_fps, 3), "decode_fps": round(plain_dec_fps, 3),

@@ -229,6 +229,32 @@ void prores_encode_job_destroy(prores_encode_job *job);
  * ms[i] for up to cap kernels; returns the count. */
 int prores_job_kernel_times(const void *job, int is_encode, const char **names, float *ms, int cap);
 
+/* Launch shapes and host pipeline depth. No reference counterpart: the
+ * crate's only knob of this kind is Config/Decoder `threads`
+ * (src/encode.rs:155-158, src/decode.rs:48-56), which likewise never changes
+ * an output. None of these changes any decoded sample or encoded byte;
+ * rivet_prores_b200.autotune times them on the device at hand. */
+typedef struct prores_tuning {
+    /* Rate-control costing runs a lane per slice component when the batch
+     * has at least this many components per SM, else a warp per component. */
+    int32_t cost_lane_items_per_sm;
+    /* Entropy decoder: warps per block (1-16), resident blocks per SM (0 =
+     * as many as fit), and slice components a lane takes per grab of the
+     * shared work counter (1, 2 or 4). */
+    int32_t entropy_warps_per_block;
+    int32_t entropy_blocks_per_sm;
+    int32_t entropy_components_per_lane;
+    /* Batches a caller keeps in flight when it streams host buffers through
+     * jobs (1-64): stored for the caller, read by no kernel. */
+    int32_t staging_depth;
+} prores_tuning;
+
+void prores_tuning_default(prores_tuning *t);
+/* Applies to the launches that follow on ctx; a job's CUDA graph keeps the
+ * shapes it was captured with. PRORES_CONFIG for a value out of range. */
+int prores_set_tuning(prores_ctx *ctx, const prores_tuning *t);
+int prores_get_tuning(prores_ctx *ctx, prores_tuning *t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,7 @@ from ._abi import Buf_, Config_, Frame_, FrameHeader_
 
 __all__ = [
     "AlphaType", "ChromaFormat", "Config", "Decoder", "Encoder", "Error", "Frame", "FrameHeader",
-    "Interlace", "Metadata", "Plane", "Profile", "context",
+    "Interlace", "Metadata", "Plane", "Profile", "Tuning", "context",
 ]
 
 
@@ -340,14 +340,52 @@ class Config:
 
 # ------------------------------------------------------------------ device
 
+@dataclass
+class Tuning:
+    """Launch shapes and host pipeline depth (prores_tuning in the C ABI).
+    None of them changes an output; `autotune` picks them per GPU."""
+
+    cost_lane_items_per_sm: int = 1024
+    entropy_warps_per_block: int = 8
+    entropy_blocks_per_sm: int = 0
+    entropy_components_per_lane: int = 1
+    staging_depth: int = 4
+
+    def _c(self) -> "_abi.Tuning_":
+        t = _abi.Tuning_()
+        for k in self.__dataclass_fields__:
+            setattr(t, k, int(getattr(self, k)))
+        return t
+
+    @staticmethod
+    def _from_c(t: "_abi.Tuning_") -> "Tuning":
+        return Tuning(**{k: int(getattr(t, k)) for k in Tuning.__dataclass_fields__})
+
+
 class Context:
-    """A device context (workspaces and streams) of libprores_b200."""
+    """A device context (workspaces and streams) of libprores_b200. On
+    creation it takes the tuning the autotuner cached for this GPU, if any."""
 
     def __init__(self, device: int = 0):
         self.device = device
         self.handle = _abi.lib().prores_create(device)
         if not self.handle:
             raise Error.Device(_abi.last_error())
+        from . import autotune
+
+        cached = autotune.load(device)
+        if cached is not None:
+            self.set_tuning(cached)
+
+    @property
+    def tuning(self) -> Tuning:
+        t = _abi.Tuning_()
+        _check(_abi.lib().prores_get_tuning(self.handle, ctypes.byref(t)))
+        return Tuning._from_c(t)
+
+    def set_tuning(self, tuning: Tuning) -> None:
+        t = tuning._c()
+        _check(_abi.lib().prores_set_tuning(self.handle, ctypes.byref(t)))
 
     def __del__(self):
         h = getattr(self, "handle", None)

@@ -83,6 +83,16 @@ class FrameHeader_(ctypes.Structure):
     ]
 
 
+class Tuning_(ctypes.Structure):
+    _fields_ = [
+        ("cost_lane_items_per_sm", ctypes.c_int32),
+        ("entropy_warps_per_block", ctypes.c_int32),
+        ("entropy_blocks_per_sm", ctypes.c_int32),
+        ("entropy_components_per_lane", ctypes.c_int32),
+        ("staging_depth", ctypes.c_int32),
+    ]
+
+
 _lib = None
 
 
@@ -132,6 +142,9 @@ def lib():
         "prores_encode_job_destroy": (None, [vp]),
         "prores_job_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, P(ctypes.c_char_p), P(ctypes.c_float),
                                                    ctypes.c_int]),
+        "prores_tuning_default": (None, [P(Tuning_)]),
+        "prores_set_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
+        "prores_get_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

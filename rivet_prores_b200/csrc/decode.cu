@@ -444,9 +444,12 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate(DecodeLaunch d) {
     }
 }
 
-constexpr int kEntropyThreads = 256;
+constexpr int kEntropyMaxThreads = 512;
 
-__global__ void __launch_bounds__(kEntropyThreads) k_entropy(DecodeLaunch d) {
+// Persistent: each warp takes 32 x entropy_per_lane slice components per
+// grab of the work counter, a lane each in turn, component-major, until the
+// list runs out.
+__global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) {
     __shared__ uint16_t run_tab[kRunTableWords];
     __shared__ uint16_t level_tab[kLevelTableWords];
     for (uint32_t i = threadIdx.x; i < kRunTableWords / 2; i += blockDim.x)
@@ -456,15 +459,19 @@ __global__ void __launch_bounds__(kEntropyThreads) k_entropy(DecodeLaunch d) {
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint32_t items = 4u * d.n_slices;
+    const uint32_t per_lane = d.entropy_per_lane > 0 ? d.entropy_per_lane : 1u;
+    const uint32_t grab = 32u * per_lane;
     for (;;) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(d.work_counter, 32u);
+        if (lane == 0) base = atomicAdd(d.work_counter, grab);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= items) break;
-        const uint32_t item = base + lane;
-        if (item < items) {
-            const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
-            decode_item(d, comp, s, run_tab, level_tab);
+        for (uint32_t k = 0; k < per_lane; k++) {
+            const uint32_t item = base + 32u * k + lane;
+            if (item < items) {
+                const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
+                decode_item(d, comp, s, run_tab, level_tab);
+            }
         }
         __syncwarp();
     }
@@ -681,9 +688,9 @@ cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_entropy(const DecodeLaunch &d, int grid, cudaStream_t s) {
+cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cudaStream_t s) {
     if (d.n_slices == 0) return cudaSuccess;
-    k_entropy<<<grid, kEntropyThreads, 0, s>>>(d);
+    k_entropy<<<shape.grid, 32 * shape.warps_per_block, 0, s>>>(d);
     return cudaGetLastError();
 }
 
@@ -707,11 +714,12 @@ cudaError_t configure_decode_kernels() {
     return upload_scans();
 }
 
-int entropy_grid(int device) {
-    int sms = 0, per_sm = 0;
+int entropy_grid(int device, int warps_per_block, int blocks_per_sm) {
+    int sms = 0, fit = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_entropy, kEntropyThreads, 0);
-    if (per_sm < 1) per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_entropy, 32 * warps_per_block, 0);
+    if (fit < 1) fit = 1;
+    const int per_sm = blocks_per_sm > 0 && blocks_per_sm < fit ? blocks_per_sm : fit;
     return sms * per_sm;
 }
 

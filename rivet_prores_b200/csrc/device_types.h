@@ -96,14 +96,23 @@ struct DecodeLaunch {
     const uint8_t *weights;  // [set][2][64] raster weights
     unsigned int *work_counter;
     uint32_t n_frames, n_pics, n_slices;
+    uint32_t entropy_per_lane;  // slice components a lane decodes per grab of the work counter
     DeviceTables tables;
+};
+
+// Launch shapes of the entropy decoder: none changes any output.
+struct EntropyShape {
+    int warps_per_block;  // 1-16
+    int grid;             // resident blocks in all
 };
 
 // Kernel launch wrappers (decode.cu). Each returns the launch's error.
 cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s);
-cudaError_t launch_entropy(const DecodeLaunch &d, int grid, cudaStream_t s);
+cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cudaStream_t s);
 cudaError_t launch_idct(const DecodeLaunch &d, cudaStream_t s);
 cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s);
-int entropy_grid(int device);
+// The grid that keeps blocks_per_sm blocks of warps_per_block warps
+// resident on every SM (0: as many as fit).
+int entropy_grid(int device, int warps_per_block, int blocks_per_sm);
 
 }  // namespace prores

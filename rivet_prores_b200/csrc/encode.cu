@@ -1279,7 +1279,11 @@ cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s) {
 // One lane per item when the batch has enough items to fill the GPU that
 // way (a lane's walk is long, so it needs the whole machine's worth of
 // them); otherwise a warp per item.
-static bool lane_mode(const EncodeLaunch &e) { return 3ull * e.n_slices >= 1024ull * (uint64_t)e.sm_count; }
+// A lane per slice component needs enough of them to fill the GPU; below
+// that, a warp per component.
+static bool lane_mode(const EncodeLaunch &e) {
+    return 3ull * e.n_slices >= (uint64_t)e.lane_items_per_sm * (uint64_t)e.sm_count;
+}
 
 cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;

@@ -317,6 +317,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     e.n_slices = plan.n_slices;
     e.any_alpha = plan.any_alpha;
     e.sm_count = ctx.sm_count;
+    e.lane_items_per_sm = ctx.current_tuning().cost_lane_items_per_sm;
     return e;
 }
 

@@ -119,6 +119,7 @@ struct EncodeLaunch {
     uint32_t n_frames, n_pics, n_slices;
     int any_alpha;
     int sm_count;
+    int lane_items_per_sm;  // a lane per slice component when 3 n_slices >= this x sm_count
 };
 
 cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s);

@@ -108,6 +108,16 @@ void Context::release(std::unique_ptr<Workspace> ws) {
     free_ws.push_back(std::move(ws));
 }
 
+Tuning Context::current_tuning() {
+    std::lock_guard<std::mutex> g(m);
+    return tuning;
+}
+
+EntropyShape Context::current_entropy() {
+    std::lock_guard<std::mutex> g(m);
+    return entropy;
+}
+
 Context::~Context() {
     cudaSetDevice(device);
     free_ws.clear();
@@ -320,6 +330,7 @@ DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan 
     d.n_frames = (uint32_t)plan.fdesc.size();
     d.n_pics = (uint32_t)plan.pdesc.size();
     d.n_slices = plan.n_slices;
+    d.entropy_per_lane = (uint32_t)ctx.current_tuning().entropy_components_per_lane;
     d.tables = ctx.tables;
     return d;
 }
@@ -331,7 +342,7 @@ Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaS
     if ((st = record_kernel(kt, "start", s))) return st;
     PR_CUDA(launch_locate(d, s), "k_locate");
     if ((st = record_kernel(kt, "k_locate", s))) return st;
-    PR_CUDA(launch_entropy(d, ctx.entropy_grid, s), "k_entropy");
+    PR_CUDA(launch_entropy(d, ctx.current_entropy(), s), "k_entropy");
     if ((st = record_kernel(kt, "k_entropy", s))) return st;
     PR_CUDA(launch_idct(d, s), "k_idct");
     if ((st = record_kernel(kt, "k_idct", s))) return st;
@@ -491,8 +502,48 @@ prores_ctx *prores_create(int device) {
         delete ctx;
         return nullptr;
     }
-    ctx->impl.entropy_grid = entropy_grid(device);
+    ctx->impl.entropy = EntropyShape{ctx->impl.tuning.entropy_warps_per_block,
+                                     entropy_grid(device, ctx->impl.tuning.entropy_warps_per_block,
+                                                  ctx->impl.tuning.entropy_blocks_per_sm)};
     return ctx;
+}
+
+void prores_tuning_default(prores_tuning *t) {
+    if (!t) return;
+    const Tuning d;
+    t->cost_lane_items_per_sm = d.cost_lane_items_per_sm;
+    t->entropy_warps_per_block = d.entropy_warps_per_block;
+    t->entropy_blocks_per_sm = d.entropy_blocks_per_sm;
+    t->entropy_components_per_lane = d.entropy_components_per_lane;
+    t->staging_depth = d.staging_depth;
+}
+
+int prores_set_tuning(prores_ctx *ctx, const prores_tuning *t) {
+    if (!ctx || !t) return fail(make_status(PRORES_CONFIG, "no context or tuning"));
+    if (t->cost_lane_items_per_sm < 0 || t->entropy_warps_per_block < 1 || t->entropy_warps_per_block > 16 ||
+        t->entropy_blocks_per_sm < 0 || t->entropy_blocks_per_sm > 32 ||
+        !(t->entropy_components_per_lane == 1 || t->entropy_components_per_lane == 2 ||
+          t->entropy_components_per_lane == 4) ||
+        t->staging_depth < 1 || t->staging_depth > 64)
+        return fail(make_status(PRORES_CONFIG, "tuning value out of range"));
+    cudaSetDevice(ctx->impl.device);
+    const int grid = entropy_grid(ctx->impl.device, t->entropy_warps_per_block, t->entropy_blocks_per_sm);
+    std::lock_guard<std::mutex> g(ctx->impl.m);
+    ctx->impl.tuning = Tuning{t->cost_lane_items_per_sm, t->entropy_warps_per_block, t->entropy_blocks_per_sm,
+                              t->entropy_components_per_lane, t->staging_depth};
+    ctx->impl.entropy = EntropyShape{t->entropy_warps_per_block, grid};
+    return PRORES_OK;
+}
+
+int prores_get_tuning(prores_ctx *ctx, prores_tuning *t) {
+    if (!ctx || !t) return fail(make_status(PRORES_CONFIG, "no context or tuning"));
+    const Tuning c = ctx->impl.current_tuning();
+    t->cost_lane_items_per_sm = c.cost_lane_items_per_sm;
+    t->entropy_warps_per_block = c.entropy_warps_per_block;
+    t->entropy_blocks_per_sm = c.entropy_blocks_per_sm;
+    t->entropy_components_per_lane = c.entropy_components_per_lane;
+    t->staging_depth = c.staging_depth;
+    return PRORES_OK;
 }
 
 void prores_destroy(prores_ctx *ctx) { delete ctx; }

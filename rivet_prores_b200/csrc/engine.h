@@ -53,12 +53,26 @@ struct KernelTimes {
     std::vector<float> ms;
 };
 
+// Launch shapes and pipeline depth (prores_tuning); none changes any output.
+struct Tuning {
+    int cost_lane_items_per_sm = 1024;
+    int entropy_warps_per_block = 8;
+    int entropy_blocks_per_sm = 0;
+    int entropy_components_per_lane = 1;
+    int staging_depth = 4;
+};
+
 struct Context {
     int device = 0;
     int sm_count = 0;
-    int entropy_grid = 0;
     DeviceTables tables{};
     std::mutex m;
+    // Read by every plan, under the mutex: a launch takes the shapes of the
+    // moment; a CUDA graph keeps those it was captured with.
+    Tuning tuning;
+    EntropyShape entropy{8, 0};
+    Tuning current_tuning();
+    EntropyShape current_entropy();
     std::vector<std::unique_ptr<Workspace>> free_ws;
     std::unique_ptr<Workspace> acquire();
     void release(std::unique_ptr<Workspace> ws);

@@ -41,7 +41,7 @@ constexpr size_t kDescBytes = 4 << 10;     // frame and picture descriptors, sta
 struct DeviceSetup {
     bool done = false;
     unsigned char *base = nullptr;  // device address of g_scratch on this device
-    int entropy_grid = 0;
+    EntropyShape entropy{8, 0};  // the library's default shape
 };
 
 std::mutex g_lock;
@@ -78,7 +78,7 @@ Status setup(int device, DeviceSetup **out) {
                 cudaSuccess)
             return cuda_status(e, "upload of the decode tables");
         d.base = base;
-        d.entropy_grid = entropy_grid(device);
+        d.entropy = EntropyShape{8, entropy_grid(device, 8, 0)};
         d.done = true;
     }
     *out = &d;
@@ -251,10 +251,11 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
     d.n_frames = 1;
     d.n_pics = n_pics;
     d.n_slices = n_slices;
+    d.entropy_per_lane = 1;
     d.tables.run_decode = reinterpret_cast<uint16_t *>(base);
     d.tables.level_decode = reinterpret_cast<uint16_t *>(base + 2 * kRunTableWords);
     d.tables.basis = reinterpret_cast<float *>(base + 2 * (kRunTableWords + kLevelTableWords));
-    if ((e = launch_locate(d, s)) != cudaSuccess || (e = launch_entropy(d, dev->entropy_grid, s)) != cudaSuccess ||
+    if ((e = launch_locate(d, s)) != cudaSuccess || (e = launch_entropy(d, dev->entropy, s)) != cudaSuccess ||
         (e = launch_idct(d, s)) != cudaSuccess || (e = launch_status(d, s)) != cudaSuccess)
         return finish(cuda_status(e, "decode launch"));
     PicStatus ps[2]{};
