@@ -349,9 +349,9 @@ static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_
         if (ef.alpha_samples) add(alpha, in[i].alpha, 2 * fd.alpha_in_off, 2 * ef.alpha_samples);
     }
     for (const Run &r : planes)
-        PR_CUDA(cudaMemcpyAsync(ws.enc_in.as<uint8_t>() + r.dst, r.src, r.len, cudaMemcpyHostToDevice, s), "frame upload");
+        PR_CUDA(ws.stager.h2d(ws.enc_in.as<uint8_t>() + r.dst, r.src, r.len, s), "frame upload");
     for (const Run &r : alpha)
-        PR_CUDA(cudaMemcpyAsync(ws.enc_alpha_in.as<uint8_t>() + r.dst, r.src, r.len, cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.enc_alpha_in.as<uint8_t>() + r.dst, r.src, r.len, s),
                 "alpha upload");
     return Status();
 }
@@ -375,23 +375,19 @@ Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores
         PR_CUDA(ws.enc_alpha_bits.reserve(4 * (plan.fdesc.size() + 1)), "cudaMalloc");
         PR_CUDA(ws.enc_alpha_bytes.reserve(8 * (plan.fdesc.size() + 1)), "cudaMalloc");
         if (!plan.fdesc.empty())
-            PR_CUDA(cudaMemcpyAsync(ws.frames.p, plan.fdesc.data(), sizeof(EncFrameDesc) * plan.fdesc.size(),
-                                    cudaMemcpyHostToDevice, s),
+            PR_CUDA(ws.stager.h2d(ws.frames.p, plan.fdesc.data(), sizeof(EncFrameDesc) * plan.fdesc.size(), s),
                     "upload");
         if (!plan.pdesc.empty())
-            PR_CUDA(cudaMemcpyAsync(ws.pics.p, plan.pdesc.data(), sizeof(EncPicDesc) * plan.pdesc.size(),
-                                    cudaMemcpyHostToDevice, s),
+            PR_CUDA(ws.stager.h2d(ws.pics.p, plan.pdesc.data(), sizeof(EncPicDesc) * plan.pdesc.size(), s),
                     "upload");
         if (!plan.sdesc.empty())
-            PR_CUDA(cudaMemcpyAsync(ws.slices.p, plan.sdesc.data(), sizeof(EncSliceDesc) * plan.sdesc.size(),
-                                    cudaMemcpyHostToDevice, s),
+            PR_CUDA(ws.stager.h2d(ws.slices.p, plan.sdesc.data(), sizeof(EncSliceDesc) * plan.sdesc.size(), s),
                     "upload");
         if (!plan.quant.empty())
-            PR_CUDA(cudaMemcpyAsync(ws.weights.p, plan.quant.data(), 4 * plan.quant.size(), cudaMemcpyHostToDevice, s),
+            PR_CUDA(ws.stager.h2d(ws.weights.p, plan.quant.data(), 4 * plan.quant.size(), s),
                     "upload");
         if (!plan.headers.empty())
-            PR_CUDA(cudaMemcpyAsync(ws.enc_frame_out.p, plan.headers.data(), plan.headers.size(),
-                                    cudaMemcpyHostToDevice, s),
+            PR_CUDA(ws.stager.h2d(ws.enc_frame_out.p, plan.headers.data(), plan.headers.size(), s),
                     "upload");
     }
     return upload_frames(ws, plan, in, s);
@@ -436,13 +432,18 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
                     int *status, Status *first_err) {
     const size_t nf = plan.fdesc.size();
     for (int attempt = 0; attempt < 2; attempt++) {
+        // Through pinned memory: a copy into pageable memory would hold up
+        // other host threads' CUDA calls until the encode is done.
+        PR_CUDA(ws.host_small.reserve(12 * (nf + 1)), "cudaMallocHost");
+        uint64_t *sizes = static_cast<uint64_t *>(ws.host_small.p);
+        uint32_t *flags = reinterpret_cast<uint32_t *>(sizes + nf);
         if (nf) {
-            PR_CUDA(cudaMemcpyAsync(plan.frame_size.data(), ws.enc_alpha_bytes.p, 8 * nf, cudaMemcpyDeviceToHost, s),
-                    "size download");
-            PR_CUDA(cudaMemcpyAsync(plan.frame_status.data(), ws.enc_alpha_bits.p, 4 * nf, cudaMemcpyDeviceToHost, s),
-                    "size download");
+            PR_CUDA(cudaMemcpyAsync(sizes, ws.enc_alpha_bytes.p, 8 * nf, cudaMemcpyDeviceToHost, s), "size download");
+            PR_CUDA(cudaMemcpyAsync(flags, ws.enc_alpha_bits.p, 4 * nf, cudaMemcpyDeviceToHost, s), "size download");
         }
         PR_CUDA(cudaStreamSynchronize(s), "encode");
+        std::copy(sizes, sizes + nf, plan.frame_size.begin());
+        std::copy(flags, flags + nf, plan.frame_status.begin());
         bool over = false;
         for (size_t f = 0; f < nf; f++) over = over || plan.frame_status[f];
         if (!over) break;
@@ -457,7 +458,7 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
         }
         plan.out_total = total;
         PR_CUDA(ws.enc_out.reserve(plan.out_total + 64), "cudaMalloc output");
-        PR_CUDA(cudaMemcpyAsync(ws.frames.p, plan.fdesc.data(), sizeof(EncFrameDesc) * nf, cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.frames.p, plan.fdesc.data(), sizeof(EncFrameDesc) * nf, s),
                 "upload");
         if (plan.graph) {
             cudaGraphExecDestroy(plan.graph);

@@ -82,6 +82,88 @@ PinnedBuf::~PinnedBuf() {
     if (p) cudaFreeHost(p);
 }
 
+bool is_page_locked(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+Stager::~Stager() {
+    for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+}
+
+cudaError_t Stager::slot(int &i) {
+    if (!buf.p) {
+        cudaError_t e = buf.reserve(kSlots * kChunk);
+        if (e != cudaSuccess) return e;
+        for (auto &x : ev)
+            if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    i = (int)(issued % kSlots);
+    if (issued >= (uint64_t)kSlots) {
+        cudaError_t e = cudaEventSynchronize(ev[i]);
+        if (e != cudaSuccess) return e;
+        if (pend[i].dst) memcpy(pend[i].dst, static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk, pend[i].len);
+    }
+    pend[i] = Pending{};
+    return cudaSuccess;
+}
+
+cudaError_t Stager::h2d(void *dst, const void *src, size_t len, cudaStream_t s) {
+    if (!len) return cudaSuccess;
+    if (is_page_locked(src)) return cudaMemcpyAsync(dst, src, len, cudaMemcpyHostToDevice, s);
+    for (size_t off = 0; off < len; off += kChunk) {
+        const size_t n = len - off < kChunk ? len - off : kChunk;
+        int i;
+        cudaError_t e = slot(i);
+        if (e != cudaSuccess) return e;
+        uint8_t *chunk = static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk;
+        memcpy(chunk, static_cast<const uint8_t *>(src) + off, n);
+        if ((e = cudaMemcpyAsync(static_cast<uint8_t *>(dst) + off, chunk, n, cudaMemcpyHostToDevice, s)) !=
+                cudaSuccess ||
+            (e = cudaEventRecord(ev[i], s)) != cudaSuccess)
+            return e;
+        issued++;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Stager::d2h(void *dst, const void *src, size_t len, cudaStream_t s) {
+    if (!len) return cudaSuccess;
+    if (is_page_locked(dst)) return cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToHost, s);
+    for (size_t off = 0; off < len; off += kChunk) {
+        const size_t n = len - off < kChunk ? len - off : kChunk;
+        int i;
+        cudaError_t e = slot(i);
+        if (e != cudaSuccess) return e;
+        uint8_t *chunk = static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk;
+        if ((e = cudaMemcpyAsync(chunk, static_cast<const uint8_t *>(src) + off, n, cudaMemcpyDeviceToHost, s)) !=
+                cudaSuccess ||
+            (e = cudaEventRecord(ev[i], s)) != cudaSuccess)
+            return e;
+        pend[i] = Pending{static_cast<uint8_t *>(dst) + off, n};
+        issued++;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Stager::finish() {
+    const uint64_t first = issued > (uint64_t)kSlots ? issued - kSlots : 0;
+    for (uint64_t k = first; k < issued; k++) {
+        const int i = (int)(k % kSlots);
+        if (!pend[i].dst) continue;
+        cudaError_t e = cudaEventSynchronize(ev[i]);
+        if (e != cudaSuccess) return e;
+        memcpy(pend[i].dst, static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk, pend[i].len);
+        pend[i] = Pending{};
+    }
+    return cudaSuccess;
+}
+
 Workspace::~Workspace() {
     if (stream) cudaStreamDestroy(stream);
 }
@@ -274,7 +356,7 @@ Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &
 Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s) {
     (void)in;
     for (const auto &c : plan.copies)
-        PR_CUDA(cudaMemcpyAsync(ws.bits.as<uint8_t>() + c.dst, c.src, c.len, cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.bits.as<uint8_t>() + c.dst, c.src, c.len, s),
                 "bitstream upload");
     return Status();
 }
@@ -297,18 +379,16 @@ Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaSt
     PR_CUDA(ws.coef.reserve(8 * (plan.coef_total + 64)), "cudaMalloc coefficient lists");
     PR_CUDA(ws.coef_count.reserve(4 * 3 * ((size_t)plan.n_slices + 1)), "cudaMalloc");
     if (!plan.fdesc.empty())
-        PR_CUDA(cudaMemcpyAsync(ws.frames.p, plan.fdesc.data(), sizeof(FrameDesc) * plan.fdesc.size(),
-                                cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.frames.p, plan.fdesc.data(), sizeof(FrameDesc) * plan.fdesc.size(), s),
                 "upload");
     if (!plan.pdesc.empty())
-        PR_CUDA(cudaMemcpyAsync(ws.pics.p, plan.pdesc.data(), sizeof(PicDesc) * plan.pdesc.size(),
-                                cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.pics.p, plan.pdesc.data(), sizeof(PicDesc) * plan.pdesc.size(), s),
                 "upload");
     if (!plan.weights.empty())
-        PR_CUDA(cudaMemcpyAsync(ws.weights.p, plan.weights.data(), plan.weights.size(), cudaMemcpyHostToDevice, s),
+        PR_CUDA(ws.stager.h2d(ws.weights.p, plan.weights.data(), plan.weights.size(), s),
                 "upload");
-    // Pageable descriptor vectors: the copies above are staged by the
-    // driver before returning, so the plan may change afterwards.
+    // The descriptor vectors are pageable: the stager copies them into
+    // pinned chunks before returning, so the plan may change afterwards.
     return Status();
 }
 
@@ -353,9 +433,11 @@ Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaS
 
 Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
                     Status *first_err) {
-    std::vector<PicStatus> ps(plan.pdesc.size());
-    if (!ps.empty())
-        PR_CUDA(cudaMemcpyAsync(ps.data(), ws.pic_status.p, sizeof(PicStatus) * ps.size(), cudaMemcpyDeviceToHost, s),
+    const size_t n_pics = plan.pdesc.size();
+    PR_CUDA(ws.host_small.reserve(sizeof(PicStatus) * (n_pics + 1)), "cudaMallocHost");
+    PicStatus *ps_host = static_cast<PicStatus *>(ws.host_small.p);
+    if (n_pics)
+        PR_CUDA(cudaMemcpyAsync(ps_host, ws.pic_status.p, sizeof(PicStatus) * n_pics, cudaMemcpyDeviceToHost, s),
                 "status download");
     // Planes straight into the caller's buffers (one copy per run of
     // host-adjacent frames).
@@ -397,9 +479,10 @@ Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prore
     }
     for (const Run &r : runs) {
         const uint16_t *src = (r.alpha ? ws.alpha.as<uint16_t>() : ws.planes.as<uint16_t>()) + r.src;
-        PR_CUDA(cudaMemcpyAsync(r.dst, src, 2 * r.len, cudaMemcpyDeviceToHost, s), "plane download");
+        PR_CUDA(ws.stager.d2h(r.dst, src, 2 * r.len, s), "plane download");
     }
     PR_CUDA(cudaStreamSynchronize(s), "decode");
+    PR_CUDA(ws.stager.finish(), "plane download");
     std::vector<Status> errs(n);
     for (int i = 0; i < n; i++) {
         const DecodeFrame &f = plan.frames[i];
@@ -418,7 +501,7 @@ Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prore
             o.transfer_characteristic = h.transfer_characteristic;
             o.matrix_coefficients = h.matrix_coefficients;
             for (uint32_t p = 0; p < f.n_pics && !st; p++) {
-                const PicStatus &q = ps[f.first_pic + p];
+                const PicStatus &q = ps_host[f.first_pic + p];
                 if (q.locate_slice >= 0)
                     st = make_status(PRORES_INVALID, "a slice runs past picture_size");
                 else if (q.slot >= 0)
@@ -709,8 +792,7 @@ int prores_decode_job_upload(prores_decode_job *job, const prores_buf *in, int n
             run_len += in[i].len;
         } else {
             if (run_src) {
-                Status st = cuda_status(cudaMemcpyAsync(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len,
-                                                        cudaMemcpyHostToDevice, s),
+                Status st = cuda_status(job->ws->stager.h2d(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len, s),
                                         "bitstream upload");
                 if (st) return fail(st);
             }
@@ -722,7 +804,7 @@ int prores_decode_job_upload(prores_decode_job *job, const prores_buf *in, int n
     }
     if (run_src) {
         Status st = cuda_status(
-            cudaMemcpyAsync(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len, cudaMemcpyHostToDevice, s),
+            job->ws->stager.h2d(job->ws->bits.as<uint8_t>() + run_dst, run_src, run_len, s),
             "bitstream upload");
         if (st) return fail(st);
     }

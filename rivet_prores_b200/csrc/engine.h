@@ -34,6 +34,33 @@ struct PinnedBuf {
     ~PinnedBuf();
 };
 
+// Copies between the device and host memory that may be pageable. Page-
+// locked memory is copied straight (asynchronously); pageable memory goes
+// through a ring of pinned chunks, because a CUDA copy to or from pageable
+// memory returns only when it is done and holds up other host threads' CUDA
+// calls meanwhile. Chunks read back are copied out by finish().
+struct Stager {
+    static constexpr int kSlots = 4;
+    static constexpr size_t kChunk = 8u << 20;
+    PinnedBuf buf;
+    cudaEvent_t ev[kSlots] = {};
+    struct Pending {
+        uint8_t *dst = nullptr;  // host destination of a chunk read back
+        size_t len = 0;
+    } pend[kSlots];
+    uint64_t issued = 0;
+    ~Stager();
+    cudaError_t h2d(void *dst, const void *src, size_t len, cudaStream_t s);
+    cudaError_t d2h(void *dst, const void *src, size_t len, cudaStream_t s);
+    // Waits for the chunks still read back and copies them out.
+    cudaError_t finish();
+
+  private:
+    cudaError_t slot(int &i);  // the next slot, free for the host
+};
+
+bool is_page_locked(const void *p);
+
 // Per-call device state: a stream and the buffers a batch needs.
 struct Workspace {
     int device = 0;
@@ -43,6 +70,11 @@ struct Workspace {
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
     PinnedBuf host_stage;
+    // Statuses and sizes read back each call. Pinned, because a copy into
+    // pageable memory returns only when done and keeps other host threads'
+    // CUDA calls waiting meanwhile.
+    PinnedBuf host_small;
+    Stager stager;
     ~Workspace();
 };
 
