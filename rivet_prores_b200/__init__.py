@@ -447,12 +447,14 @@ class Decoder:
             raise r
         return r
 
-    def decode_batch(self, datas: Sequence[bytes]) -> List[Union[Frame, Error]]:
+    def decode_batch(self, datas: Sequence[bytes], alloc=None) -> List[Union[Frame, Error]]:
         """Decodes every frame in one batched launch; each entry is a Frame or
-        the Error that frame gave."""
+        the Error that frame gave. `alloc(n, dtype)`, when given, makes the
+        output arrays (for example from a pool of page-locked buffers, which
+        the planes then reach by DMA with no host copy)."""
         L = _abi.lib()
         n = len(datas)
-        datas = [bytes(d) for d in datas]
+        alloc = alloc or np.empty
         depth = self.bit_depth or 0
         bufs = (Buf_ * max(n, 1))()
         outs = (Frame_ * max(n, 1))()
@@ -461,14 +463,14 @@ class Decoder:
         arrays = [None] * n
         keep = []
         for i, d in enumerate(datas):
-            arr = (ctypes.c_uint8 * max(len(d), 1)).from_buffer_copy(d if d else b"\0")
-            keep.append(arr)
-            bufs[i].data = ctypes.cast(arr, ctypes.POINTER(ctypes.c_uint8))
+            a = _as_u8(d) if len(d) else np.zeros(1, np.uint8)
+            keep.append(a)
+            bufs[i].data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
             bufs[i].len = len(d)
             info = Frame_()
-            if L.prores_probe(d, len(d), depth, ctypes.byref(info)) == _abi.OK:
-                data = np.empty(info.data_len, np.uint16)
-                alpha = np.empty(info.alpha_len, np.uint16) if info.alpha_len else None
+            if L.prores_probe(a.ctypes.data_as(ctypes.c_char_p), len(d), depth, ctypes.byref(info)) == _abi.OK:
+                data = alloc(info.data_len, np.uint16)
+                alpha = alloc(info.alpha_len, np.uint16) if info.alpha_len else None
                 outs[i].data, outs[i].data_len = _ptr16(data), info.data_len
                 if alpha is not None:
                     outs[i].alpha, outs[i].alpha_len = _ptr16(alpha), info.alpha_len
@@ -559,9 +561,11 @@ class Encoder:
 # ------------------------------------------------------------------ resident jobs
 
 def _as_u8(x) -> np.ndarray:
+    """A uint8 view of x's bytes (no copy for bytes, bytearray, memoryview
+    or arrays)."""
     if isinstance(x, np.ndarray):
         return x if x.dtype == np.uint8 else x.view(np.uint8)
-    return np.frombuffer(bytes(x), dtype=np.uint8)
+    return np.frombuffer(x, dtype=np.uint8)
 
 
 def _stream_ptr(stream) -> Optional[int]:

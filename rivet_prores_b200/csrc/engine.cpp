@@ -44,12 +44,21 @@ Status cuda_status(cudaError_t e, const char *what) {
         if (st_) return st_;                                  \
     } while (0)
 
+// Capacity for `bytes`: at least half as much again as asked and a whole
+// number of MiB, so that a workspace serving batches of changing sizes
+// settles after a few growths (each reallocation waits for the device).
+static size_t grown(size_t bytes, size_t cap) {
+    size_t want = bytes + bytes / 2 + 4096;
+    if (want < cap + cap / 2) want = cap + cap / 2;
+    return (want + (1u << 20) - 1) & ~(size_t)((1u << 20) - 1);
+}
+
 cudaError_t DeviceBuf::reserve(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
+    const size_t want = grown(bytes, cap);
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    size_t want = bytes + bytes / 8 + 256;
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -65,10 +74,10 @@ DeviceBuf::~DeviceBuf() {
 
 cudaError_t PinnedBuf::reserve(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
+    const size_t want = grown(bytes, cap);
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    size_t want = bytes + bytes / 8 + 4096;
     cudaError_t e = cudaMallocHost(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;

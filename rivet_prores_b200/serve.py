@@ -60,15 +60,95 @@ def encode_cost(frame, config) -> int:
     return 6 * n + int(target) + alpha + 4096
 
 
-class GpuBackend:
-    """The library's batched calls."""
+class _Lease:
+    """Exposes one pooled block to numpy; the block goes back to its pool
+    when the lease (the base of every array made from it) is collected."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, mv: memoryview):
+        self.mv = mv
+
+    def __buffer__(self, flags):
+        return self.mv
+
+    def __release_buffer__(self, view):
+        pass
+
+
+def _pinned_block(size: int) -> np.ndarray:
+    import torch
+
+    return torch.empty(size, dtype=torch.uint8, pin_memory=True).numpy()
+
+
+class PinnedPool:
+    """Reusable page-locked host buffers for decoded planes.
+
+    Fresh host memory costs a page fault per 4 KB on first touch, which for
+    decoded UHD planes takes longer than the decode; pooled page-locked
+    blocks are already mapped, and the device writes them by DMA with no
+    staging copy. A block returns to the pool when the last array viewing it
+    is collected. Blocks come in 1 MiB steps; `limit` bounds the bytes kept
+    idle."""
+
+    def __init__(self, limit: int = 4 << 30, allocate: Optional[Callable[[int], np.ndarray]] = None):
+        self.limit = limit
+        self.idle = 0
+        self.made = 0
+        self.free = collections.defaultdict(list)
+        self.lock = threading.Lock()
+        self.allocate = allocate or _pinned_block
+
+    def take(self, n: int, dtype=np.uint16) -> np.ndarray:
+        import weakref
+
+        nbytes = max(1, n * np.dtype(dtype).itemsize)
+        size = (nbytes + (1 << 20) - 1) & ~((1 << 20) - 1)
+        with self.lock:
+            block = self.free[size].pop() if self.free[size] else None
+            if block is not None:
+                self.idle -= size
+        if block is None:
+            block = self.allocate(size)
+            with self.lock:
+                self.made += 1
+        lease = _Lease(memoryview(block))
+        weakref.finalize(lease, self._give, size, block)
+        return np.frombuffer(lease, dtype=np.uint8, count=nbytes).view(dtype)[:n]
+
+    def _give(self, size, block):
+        with self.lock:
+            if self.idle + size <= self.limit:
+                self.free[size].append(block)
+                self.idle += size
+
+
+def pinned_frame(frame, pool: PinnedPool):
+    """A copy of `frame` whose planes (and alpha) lie in page-locked pooled
+    memory, as a server's receive buffers would: the device then reads them
+    by DMA, with no staging copy."""
+    from . import Frame
+
+    data = pool.take(frame.data.size)
+    data[:] = frame.data
+    alpha = None
+    if frame.alpha is not None:
+        alpha = pool.take(frame.alpha.size)
+        alpha[:] = frame.alpha
+    return Frame(frame.width, frame.height, frame.bit_depth, frame.chroma, frame.interlace, frame.metadata, data,
+                 frame.planes, alpha)
+
+
+class GpuBackend:
+    """The library's batched calls; decoded planes land in a pool of
+    page-locked host buffers."""
+
+    def __init__(self, device: int = 0, pool: Optional[PinnedPool] = None):
         from . import Decoder, Encoder
 
         self.device = device
         self._Decoder = Decoder
         self._Encoder = Encoder
+        self.pool = pool if pool is not None else PinnedPool()
 
     def decode(self, reqs: List[Request]):
         by_depth = collections.defaultdict(list)
@@ -76,7 +156,8 @@ class GpuBackend:
             by_depth[r.bit_depth].append(i)
         out = [None] * len(reqs)
         for depth, idx in by_depth.items():
-            res = self._Decoder(bit_depth=depth, device=self.device).decode_batch([reqs[i].payload for i in idx])
+            res = self._Decoder(bit_depth=depth, device=self.device).decode_batch([reqs[i].payload for i in idx],
+                                                                               alloc=self.pool.take)
             for i, r in zip(idx, res):
                 out[i] = r
         return out
@@ -103,7 +184,10 @@ class Server:
         self.queue: Deque[Request] = collections.deque()
         self.cv = threading.Condition()
         self.closed = False
-        self.done: List[Request] = []
+        # (submitted, done) times of finished requests: the requests
+        # themselves are let go, so that their results live only as long as
+        # the callers keep them.
+        self.done: List[tuple] = []
         self.batches: List[int] = []
         self.peak_in_use = 0
         self.threads = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
@@ -174,15 +258,16 @@ class Server:
             with self.cv:
                 self.in_use -= sum(r.cost for r in batch)
                 self.batches.append(len(batch))
-                for i, r in enumerate(batch):
+                for r in batch:
                     r.t_done = now
-                    self.done.append(r)
+                    self.done.append((r.t_submit, now))
                 self.cv.notify_all()
             for i, r in enumerate(batch):
                 if exc is not None:
                     r.future.set_exception(exc)
                 else:
                     r.future.set_result(results[i])
+            del batch, results
 
     def close(self):
         with self.cv:
@@ -195,10 +280,10 @@ class Server:
 
     def stats(self) -> dict:
         with self.cv:
-            lat = sorted((r.t_done - r.t_submit) * 1000.0 for r in self.done)
+            lat = sorted((d - a) * 1000.0 for a, d in self.done)
             batches = list(self.batches)
-            first = min((r.t_submit for r in self.done), default=0.0)
-            last = max((r.t_done for r in self.done), default=0.0)
+            first = min((a for a, _ in self.done), default=0.0)
+            last = max((d for _, d in self.done), default=0.0)
         if not lat:
             return {"requests": 0}
         pct = lambda p: lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
@@ -212,9 +297,19 @@ def poisson_run(server: Server, make_request: Callable[[int], tuple], rate: floa
                 seed: int = 0) -> dict:
     """Submits requests at Poisson times (mean `rate` per second) for
     `seconds`; make_request(i) gives ("decode", data) or ("encode", frame,
-    config). Waits for all and returns the server's stats."""
+    config). Each result is dropped as it arrives, as a client that consumes
+    it would; waits for all and returns the server's stats."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    futures = []
+    lock = threading.Condition()
+    state = {"submitted": 0, "finished": 0, "errors": 0}
+
+    def finished(f: Future):
+        failed = f.exception() is not None
+        with lock:
+            state["finished"] += 1
+            state["errors"] += int(failed)
+            lock.notify_all()
+
     t0 = time.perf_counter()
     t = 0.0
     i = 0
@@ -227,13 +322,19 @@ def poisson_run(server: Server, make_request: Callable[[int], tuple], rate: floa
             time.sleep(delay)
         req = make_request(i)
         if req[0] == "decode":
-            futures.append(server.submit_decode(req[1]))
+            fut = server.submit_decode(req[1])
         else:
-            futures.append(server.submit_encode(req[1], req[2]))
+            fut = server.submit_encode(req[1], req[2])
+        with lock:
+            state["submitted"] += 1
+        fut.add_done_callback(finished)
+        del fut
         i += 1
-    for f in futures:
-        f.result()
+    with lock:
+        while state["finished"] < state["submitted"]:
+            lock.wait(1.0)
     s = server.stats()
     s["offered_rate"] = rate
     s["seconds"] = seconds
+    s["errors"] = state["errors"]
     return s

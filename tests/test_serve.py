@@ -5,6 +5,7 @@ order, results to the right request, failures to the batch's requests."""
 import threading
 import time
 
+import numpy as np
 import pytest
 
 from rivet_prores_b200.serve import Server, poisson_run
@@ -110,3 +111,41 @@ def test_poisson_run_reports_latency_percentiles():
     srv.close()
     assert st["requests"] > 100
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+
+
+def test_pinned_pool_reuses_a_block_only_after_every_view_is_gone():
+    import gc
+
+    from rivet_prores_b200.serve import PinnedPool
+
+    pool = PinnedPool(limit=8 << 20, allocate=lambda n: np.zeros(n, np.uint8))
+    a = pool.take(1000)
+    assert a.dtype == np.uint16 and a.size == 1000
+    a[:] = 7
+    view = a[10:20]
+    del a
+    gc.collect()
+    b = pool.take(1000)  # the first block is still viewed: a new one
+    assert pool.made == 2
+    assert (view == 7).all()
+    del view, b
+    gc.collect()
+    c = pool.take(300_000)  # the same 1 MiB class: a pooled block
+    assert pool.made == 2 and c.size == 300_000
+    d = pool.take(600_000)  # 1.2 MB: the 2 MiB class, a new block
+    assert pool.made == 3
+    del c, d
+    gc.collect()
+    assert pool.idle == 4 << 20
+
+
+def test_pinned_pool_keeps_at_most_its_limit_idle():
+    import gc
+
+    from rivet_prores_b200.serve import PinnedPool
+
+    pool = PinnedPool(limit=2 << 20, allocate=lambda n: np.zeros(n, np.uint8))
+    xs = [pool.take(100) for _ in range(5)]
+    del xs
+    gc.collect()
+    assert pool.idle == 2 << 20
