@@ -52,7 +52,7 @@ def parse_args():
                     help="parts the end-to-end batch is split over (0: the tuned staging depth)")
     ap.add_argument("--no-tune", action="store_true", help="keep the cached or default launch shapes")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=4.0, help="0 skips the serving run")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="0 skips the serving run")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean requests/s (Poisson)")
     return ap.parse_args()
 
@@ -400,9 +400,10 @@ def run_serving(args, device):
 
     pool = workloads.mixed_pool()
     packets = [P.Encoder(c, device=device).encode(f) for f, c in pool]
-    # Encode requests arrive in page-locked receive buffers.
+    # Requests arrive in page-locked receive buffers.
     receive = S.PinnedPool()
     pool = [(S.pinned_frame(f, receive), c) for f, c in pool]
+    packets = [S.pinned_bytes(p, receive) for p in packets]
 
     def maker(seed):
         rng = np.random.Generator(np.random.PCG64(seed))
@@ -416,9 +417,11 @@ def run_serving(args, device):
 
     out = {"mix": "720x486i HQ, 720p LT, 1080p Proxy/422/HQ, UHD HQ, 4096x2160 4444 (16-bit in); 70/30 decode/encode",
            "budget_bytes": 8 << 30,
-           "host_buffers": "decode: packets as bytes, planes into pooled page-locked buffers; encode: frames in "
-                           "page-locked receive buffers"}
-    for name, workers, max_batch, seconds in [("batched", 3, 64, args.serve_seconds),
+           "host_buffers": "requests (packets, frames) in page-locked receive buffers; decoded planes into "
+                           "pooled page-locked buffers"}
+    # Batches of at most 16: large enough to fill the device, small enough
+    # that a request does not wait behind a long batch.
+    for name, workers, max_batch, seconds in [("batched", 3, 16, args.serve_seconds),
                                               ("plain", 1, 1, max(1.0, args.serve_seconds / 4))]:
         # One backend (and its pool of page-locked output buffers) for the
         # warm-up and the measured run.

@@ -46,7 +46,8 @@ def decode_cost(data: bytes) -> int:
     from . import _abi
 
     info = _abi.Frame_()
-    if _abi.lib().prores_probe(data, len(data), 0, ctypes.byref(info)) != _abi.OK:
+    a = np.frombuffer(data, dtype=np.uint8) if len(data) else np.zeros(1, np.uint8)
+    if _abi.lib().prores_probe(a.ctypes.data_as(ctypes.c_char_p), len(data), 0, ctypes.byref(info)) != _abi.OK:
         return len(data) + 4096
     return len(data) + 10 * info.data_len + 2 * info.alpha_len + 4096
 
@@ -120,6 +121,13 @@ class PinnedPool:
             if self.idle + size <= self.limit:
                 self.free[size].append(block)
                 self.idle += size
+
+
+def pinned_bytes(data, pool: PinnedPool) -> np.ndarray:
+    """A copy of `data` in page-locked pooled memory (a receive buffer)."""
+    out = pool.take(len(data), np.uint8)
+    out[:] = np.frombuffer(data, dtype=np.uint8)
+    return out
 
 
 def pinned_frame(frame, pool: PinnedPool):
@@ -197,7 +205,11 @@ class Server:
     # -------------------------------------------------------------- intake
 
     def submit_decode(self, data: bytes, bit_depth: Optional[int] = None, cost: Optional[int] = None) -> Future:
-        data = bytes(data)
+        """`data`: bytes, or an array (for example a page-locked receive
+        buffer, which reaches the device by DMA) that stays unchanged until
+        the future resolves; other buffers are copied."""
+        if not isinstance(data, (bytes, np.ndarray)):
+            data = bytes(data)
         r = Request("decode", data, None, bit_depth, decode_cost(data) if cost is None else cost)
         return self._submit(r)
 
