@@ -37,6 +37,17 @@ W, H = 3840, 2160
 # Algorithmic bytes per frame and direction: the packet (3 643 238 B at the
 # 422 HQ target) plus the 16.59 M u16 samples of the planes.
 ALGO_BYTES_PER_FRAME = 3_643_238 + 2 * (W * H * 2)
+# DRAM bytes (read + write) per frame and launch, and issue-slot use, from
+# one ncu capture of 14 UHD 422 HQ frames (profiles/kernels_uhd_422hq_b14.md;
+# traffic grows with the frames a launch covers). k_cost is the mean of its
+# nine probe launches.
+PROFILED = {
+    "k_cost": {"dram_bytes_per_frame": 51.41e6, "issue_active_pct": "52-71"},
+    "k_idct": {"dram_bytes_per_frame": 73.19e6, "issue_active_pct": "59"},
+    "k_fdct": {"dram_bytes_per_frame": 97.87e6, "issue_active_pct": "38"},
+    "k_entropy": {"dram_bytes_per_frame": 70.97e6, "issue_active_pct": "46"},
+    "k_pack": {"dram_bytes_per_frame": 78.98e6, "issue_active_pct": "72"},
+}
 
 
 def parse_args():
@@ -378,7 +389,12 @@ def run_b200(args):
         "gpu_launches": launches_per_step * args.steps,
         "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(kernel_ms.items(), key=lambda x: -x[1])},
         "roofline": {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": (round(PROFILED[dominant]["dram_bytes_per_frame"] * B) if dominant in PROFILED
+                                 else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 14 frames, "
+                                       "scaled to the launch's frames (profiles/kernels_uhd_422hq_b14.md)",
+                     "issue_active_pct": PROFILED.get(dominant, {}).get("issue_active_pct"),
                      "peak_source": peak_kind,
                      "algorithmic_bytes": f"{ALGO_BYTES_PER_FRAME} B per frame (packet + u16 planes) x {B}"},
         "cpu_baseline": cpu,
