@@ -5,6 +5,7 @@
 // src/vlc.rs:28-68 and src/tables.rs:6-38 entry for entry.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 
 #if defined(__CUDACC__)
@@ -118,6 +119,17 @@ PR_HD Codebook level_book(uint32_t prev) {
 // Prefix tables for the decoder: for each context and every kDecodeBits-bit
 // window prefix, (symbol << 5) | length of the codeword it starts with, or 0
 // when that codeword is longer.
+// T[x][u] = C(u)/2 cos((2x+1) u pi / 16), computed in double and rounded
+// once to single precision (the crate's src/dct.rs:11-25). Host only.
+inline void dct_basis(float out[64]) {
+    for (int x = 0; x < 8; x++)
+        for (int u = 0; u < 8; u++) {
+            const double cu = u == 0 ? 0.70710678118654752440 : 1.0;
+            const double a = (double)((2 * x + 1) * u) * 3.14159265358979323846 / 16.0;
+            out[8 * x + u] = (float)(cu / 2.0 * cos(a));
+        }
+}
+
 static constexpr uint32_t kDecodeBits = 9;
 static constexpr uint32_t kDecodeEntries = 1u << kDecodeBits;
 static constexpr uint32_t kRunTableWords = 16 * kDecodeEntries;

@@ -39,6 +39,7 @@
 namespace prores {
 
 __constant__ uint8_t c_enc_scan[2][64];
+__constant__ float c_fdct_basis[64];  // T[x][u], the same values as the decoder's
 
 namespace {
 
@@ -79,7 +80,7 @@ __device__ __forceinline__ int32_t quantise1(float f, float inv, float r) {
 
 // ---------------------------------------------------------------- fdct
 
-constexpr int kFdctThreads = 256;
+constexpr int kFdctThreads = 128;
 constexpr int kMaxSliceCoefs = 64 * 12 * 8;
 
 __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_t mb_x, uint32_t mb_y, uint32_t m,
@@ -97,56 +98,54 @@ __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_
     }
 }
 
+// One warp per slice component, one lane per 8x8 block (a component has
+// at most 32 blocks; lanes past the component's count idle). A lane loads
+// its block's 8 rows, transforms them (rows, then columns, in the crate's
+// order; the row results wait in shared memory, lane-minor, so no bank
+// conflicts) and stores each coefficient at its scanned place
+// n * scan[k] + blk: the lanes of a component store consecutive floats.
+// The basis comes from constant memory, read by every lane at the same
+// address. A chunk of 32 scanned coefficients is one scanned position of a
+// 32-block component, or several positions of a smaller one; its largest
+// |F| is reduced over the lanes as each position is stored and kept in
+// shared memory until the component is done. (Cb and Cr of a 4:2:2 slice
+// in one warp measured slower: fewer warps to hide the loads.)
 __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
-    __shared__ float tmp[kMaxSliceCoefs];  // [comp][y][u][blk]
-    extern __shared__ __align__(16) float scanned[];  // kMaxSliceCoefs: the slice in scanned order
-    __shared__ float basis[64];
-    __shared__ uint8_t scan[64];
-    const EncSliceDesc sd = e.slices[blockIdx.x];
+    __shared__ uint32_t cmax_sh[kFdctThreads / 32][64];
+    __shared__ float tmp_sh[kFdctThreads / 32][64][32];  // the row pass, [y * 8 + u][lane]
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t item = blockIdx.x * (kFdctThreads / 32) + warp;
+    if (item >= 3u * e.n_slices) return;  // the whole warp
+    const uint32_t s = item / 3u, c = item - 3u * s;
+    const EncSliceDesc sd = e.slices[s];
     const EncPicDesc &pd = e.pics[sd.pic];
     const EncFrameDesc &fd = e.frames[pd.frame];
-    const uint32_t tid = threadIdx.x;
-    if (tid < 64) basis[tid] = e.basis[tid];
-    else if (tid < 128) scan[tid - 64] = c_enc_scan[pd.interlaced_scan][tid - 64];
-    __syncthreads();
     const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
-    const uint32_t mbs = sd.mbs;
-    uint32_t nbk[3], start[3];
-    nbk[0] = 4u * mbs;
-    nbk[1] = nbk[2] = cpm * mbs;
-    start[0] = 0;
-    start[1] = 64u * nbk[0];
-    start[2] = start[1] + 64u * nbk[1];
-    const float scale = fd.in_scale;
-
-    // Pass 1: tmp[y][u] = sum_x p[y][x] T[x][u], x in order from 0.
-    for (uint32_t c = 0; c < 3; c++) {
-        const uint32_t segs = (c == 0 || cpm == 4) ? 2u * mbs : mbs;
-        const uint32_t per_mb = c == 0 ? 4u : cpm;
+    const uint32_t per_mb = c == 0 ? 4u : cpm;
+    const uint32_t nb = per_mb * sd.mbs;
+    const uint32_t start = c == 0 ? 0u : 64u * sd.mbs * (4u + (c - 1u) * cpm);
+    uint32_t *cm = cmax_sh[warp];
+    cm[lane] = 0;
+    cm[lane + 32] = 0;
+    __syncwarp();
+    if (lane < nb) {
+        const uint8_t *scan = c_enc_scan[pd.interlaced_scan];
+        float (*tmp)[32] = tmp_sh[warp];
+        const uint32_t m = lane / per_mb, b = lane - m * per_mb;
+        uint32_t bx, by;
+        block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, b, bx, by);
         const uint32_t w = fd.plane_w[c];
         const uint16_t *plane = e.in + fd.in_off[c];
-        for (uint32_t t = tid; t < 16u * segs; t += kFdctThreads) {
-            const uint32_t r = t / segs, sx = t - r * segs;
-            uint32_t m, bb;
-            if (c == 0) {
-                m = sx >> 1;
-                bb = ((r >> 3) << 1) | (sx & 1u);
-            } else if (cpm == 2) {
-                m = sx;
-                bb = r >> 3;
-            } else {
-                m = sx >> 1;
-                bb = ((sx & 1u) << 1) | (r >> 3);
-            }
-            const uint32_t blk = m * per_mb + bb, y = r & 7u;
-            uint32_t bx, by;
-            block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, bb, bx, by);
+        const float scale = fd.in_scale;
+        // Rows: tmp[y][u] = sum_x p[y][x] T[x][u], x in order from 0.
+#pragma unroll
+        for (int y = 0; y < 8; y++) {
             // Edge replication: the last picture row and column repeat.
-            const uint32_t py = min(by + y, pd.height - 1u);
+            const uint32_t py = min(by + (uint32_t)y, pd.height - 1u);
             const uint16_t *line = plane + (uint64_t)(pd.first_row + pd.row_step * py) * w;
             float p[8];
             if (bx + 8u <= w && ((reinterpret_cast<uintptr_t>(line + bx) & 15u) == 0)) {
-                const uint4 v = *reinterpret_cast<const uint4 *>(line + bx);
+                const uint4 v = __ldg(reinterpret_cast<const uint4 *>(line + bx));
                 const uint32_t words[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
@@ -157,59 +156,45 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
 #pragma unroll
                 for (int x = 0; x < 8; x++) {
                     const uint32_t col = min(bx + (uint32_t)x, w - 1u);
-                    p[x] = __fsub_rn(__fmul_rn((float)line[col], scale), 256.0f);
+                    p[x] = __fsub_rn(__fmul_rn((float)__ldg(line + col), scale), 256.0f);
                 }
             }
-            const uint32_t nb = nbk[c];
-            float *dst = tmp + start[c];
 #pragma unroll
             for (int u = 0; u < 8; u++) {
-                float s = 0.0f;
+                float acc = 0.0f;
 #pragma unroll
-                for (int x = 0; x < 8; x++) s = __fadd_rn(s, __fmul_rn(p[x], basis[8 * x + u]));
-                dst[(y * 8u + u) * nb + blk] = s;
+                for (int x = 0; x < 8; x++) acc = __fadd_rn(acc, __fmul_rn(p[x], c_fdct_basis[8 * x + u]));
+                tmp[8 * y + u][lane] = acc;
             }
         }
-    }
-    __syncthreads();
-
-    // Pass 2: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0, put at
-    // the scanned position n * scan[8v + u] + blk of the component.
-    for (uint32_t c = 0; c < 3; c++) {
-        const uint32_t nb = nbk[c];
-        const float *src = tmp + start[c];
-        float *dst = scanned + start[c];
-        for (uint32_t t = tid; t < 8u * nb; t += kFdctThreads) {
-            const uint32_t blk = t % nb, u = t / nb;
+        // Columns: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0.
+        float *out = e.coef + sd.coef + start;
+        const uint32_t mask = nb >= 32u ? 0xffffffffu : (1u << nb) - 1u;
+#pragma unroll 1
+        for (int u = 0; u < 8; u++) {
             float col[8];
 #pragma unroll
-            for (int y = 0; y < 8; y++) col[y] = src[(y * 8u + u) * nb + blk];
+            for (int y = 0; y < 8; y++) col[y] = tmp[8 * y + u][lane];
 #pragma unroll
             for (int v = 0; v < 8; v++) {
-                float s = 0.0f;
+                float acc = 0.0f;
 #pragma unroll
-                for (int y = 0; y < 8; y++) s = __fadd_rn(s, __fmul_rn(basis[8 * y + v], col[y]));
-                dst[nb * scan[8 * v + u] + blk] = s;
+                for (int y = 0; y < 8; y++) acc = __fadd_rn(acc, __fmul_rn(c_fdct_basis[8 * y + v], col[y]));
+                const uint32_t sp = scan[8 * v + u];
+                out[nb * sp + lane] = acc;
+                // Every active lane is at this position, in one chunk.
+                const uint32_t big = __reduce_max_sync(mask, __float_as_uint(fabsf(acc)));
+                if (lane == 0) {
+                    const uint32_t j = (nb * sp) >> 5;
+                    cm[j] = max(cm[j], big);
+                }
             }
         }
     }
-    __syncthreads();
-
-    // The slice out in 16-byte stores, with the largest |F| of each chunk of
-    // 32 coefficients (eight lanes' stores). The slice holds a multiple of
-    // 512 coefficients, so whole warps take part in every shuffle.
-    const uint32_t n4 = (64u * (nbk[0] + 2u * nbk[1])) / 4u;
-    float4 *gout = reinterpret_cast<float4 *>(e.coef + sd.coef);
-    const float4 *sin = reinterpret_cast<const float4 *>(scanned);
-    for (uint32_t i = tid; i < n4; i += kFdctThreads) {
-        const float4 v = sin[i];
-        gout[i] = v;
-        float m = fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 4));
-        if ((i & 7u) == 0) e.coef_max[(sd.coef >> 5) + (i >> 3)] = m;
-    }
+    __syncwarp();
+    // The component's 2 nb chunk maxima.
+    float *cmax = e.coef_max + ((sd.coef + start) >> 5);
+    for (uint32_t j = lane; j < 2u * nb; j += 32) cmax[j] = __uint_as_float(cm[j]);
 }
 
 // ---------------------------------------------------------------- alpha
@@ -1259,7 +1244,8 @@ __global__ void __launch_bounds__(32 * kAlphaWarps) k_pack_alpha(EncodeLaunch e)
 
 cudaError_t launch_fdct(const EncodeLaunch &e, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
-    k_fdct<<<e.n_slices, kFdctThreads, 4 * kMaxSliceCoefs, s>>>(e);
+    const uint32_t warps = 3u * e.n_slices, per_block = kFdctThreads / 32;
+    k_fdct<<<(warps + per_block - 1) / per_block, kFdctThreads, 0, s>>>(e);
     return cudaGetLastError();
 }
 
@@ -1347,9 +1333,9 @@ cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
 }
 
 cudaError_t configure_encode_kernels() {
-    // 24 KB of static and 24 KB of dynamic shared memory pass the 48 KB that
-    // needs no opt-in.
-    cudaError_t err = cudaFuncSetAttribute(k_fdct, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * kMaxSliceCoefs);
+    float basis[64];
+    dct_basis(basis);
+    cudaError_t err = cudaMemcpyToSymbol(c_fdct_basis, basis, sizeof basis);
     if (err != cudaSuccess) return err;
     uint8_t sc[2][64];
     for (int i = 0; i < 64; i++) {

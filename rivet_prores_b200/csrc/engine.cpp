@@ -543,15 +543,8 @@ static Status make_tables(Context &c) {
     std::vector<uint16_t> run(kRunTableWords), level(kLevelTableWords);
     build_decode_table(run_book, 16, run.data());
     build_decode_table(level_book, 9, level.data());
-    // T[x][u] = C(u)/2 cos((2x+1) u pi / 16), computed in double and rounded
-    // once to single precision (the crate's src/dct.rs:11-25).
     float basis[64];
-    for (int x = 0; x < 8; x++)
-        for (int u = 0; u < 8; u++) {
-            const double cu = u == 0 ? 0.70710678118654752440 : 1.0;
-            const double a = (double)((2 * x + 1) * u) * 3.14159265358979323846 / 16.0;
-            basis[8 * x + u] = (float)(cu / 2.0 * cos(a));
-        }
+    dct_basis(basis);
     PR_CUDA(cudaMalloc(&c.tables.run_decode, run.size() * 2), "cudaMalloc");
     PR_CUDA(cudaMalloc(&c.tables.level_decode, level.size() * 2), "cudaMalloc");
     PR_CUDA(cudaMalloc(&c.tables.basis, sizeof basis), "cudaMalloc");
