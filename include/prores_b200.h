@@ -165,6 +165,50 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
 
 void prores_buffer_free(void *p);
 
+/* ---- frames found in a MOV, frames in device memory -------------------- */
+
+/* Where one frame lies in a buffer. */
+typedef struct prores_span {
+    size_t offset;
+    size_t len;
+} prores_span;
+
+/* The crate's scan for whole frames in a MOV file (or a prefix of one)
+ * without parsing the container (tests/sample.rs:20-38,
+ * examples/prores_bench.rs:103-121): at each byte position i from 4, "icpf"
+ * with a big-endian frame_size >= 28 at i - 4 that ends inside the data is a
+ * frame, and the scan resumes at its end. Writes up to cap spans and returns
+ * how many frames there are (which may exceed cap). */
+size_t prores_scan_frames(const uint8_t *data, size_t len, prores_span *frames, size_t cap);
+
+/* The same scan over data in device memory (d_data, len bytes): a kernel
+ * finds every "icpf" at once and the host resolves them in order by the
+ * same rule, so the spans equal prores_scan_frames's. *count gets the number
+ * of frames; up to cap spans are written. `stream` (a cudaStream_t, or NULL)
+ * orders the scan after the caller's writes of d_data. No reference
+ * counterpart for device memory. */
+int prores_scan_frames_device(prores_ctx *ctx, const uint8_t *d_data, size_t len, prores_span *frames, size_t cap,
+                              size_t *count, void *stream);
+
+/* prores_probe for n frames that lie in device memory (d_data, data_len
+ * bytes; frames[i] inside it): only the frame headers are read back.
+ * status[i] and prores_batch_error(i) as in prores_decode_batch. */
+int prores_probe_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len, const prores_span *frames, int n,
+                        uint32_t out_bit_depth, prores_frame *info, int *status);
+
+/* Decoder::decode (src/decode.rs:61-104) for n frames that lie in device
+ * memory, into the caller's device buffers: out[i].data (data_len samples,
+ * Y'‖Cb‖Cr as in prores_frame) and out[i].alpha (alpha_len samples, for a
+ * frame with alpha) are device pointers, sized as prores_probe_device
+ * says. Only the header bytes planning needs are read back to the host; the
+ * bitstreams are copied device to device and the planes written in place.
+ * The work runs on `stream` (a cudaStream_t, or NULL for the library's own)
+ * and the call returns when it is done; the metadata fields of out[i] and
+ * status[i] are filled as in prores_decode_batch. PRORES_CONFIG when a span
+ * lies outside data_len or an output buffer is too small. */
+int prores_decode_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len, const prores_span *frames, int n,
+                         uint32_t out_bit_depth, prores_frame *out, int *status, void *stream);
+
 /* ---- decode without device allocation --------------------------------- */
 
 /* Size of the fixed device array prores_decode_noalloc keeps its scratch in:

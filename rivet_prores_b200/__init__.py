@@ -24,7 +24,7 @@ from ._abi import Buf_, Config_, Frame_, FrameHeader_
 
 __all__ = [
     "AlphaType", "ChromaFormat", "Config", "Decoder", "Encoder", "Error", "Frame", "FrameHeader",
-    "Interlace", "Metadata", "Plane", "Profile", "Tuning", "context",
+    "Interlace", "Metadata", "Plane", "Profile", "Tuning", "context", "scan_frames", "DeviceFrame",
 ]
 
 
@@ -485,6 +485,112 @@ class Decoder:
                 data, alpha = arrays[i]
                 results[i] = _frame_from_c(outs[i], data, alpha)
         return results
+
+    def probe_device(self, data, frames, length: Optional[int] = None) -> List[Union["_abi.Frame_", Error]]:
+        """Sizes and metadata of frames that lie in device memory (`data`,
+        with `frames` as (offset, length) pairs); only their headers are
+        read back."""
+        n_bytes = int(length if length is not None else data.numel())
+        n = len(frames)
+        infos = (Frame_ * max(n, 1))()
+        status = (ctypes.c_int * max(n, 1))()
+        _check(_abi.lib().prores_probe_device(context(self.device).handle, _device_ptr(data), n_bytes,
+                                              _spans(frames), n, self.bit_depth or 0, infos, status))
+        return [infos[i] if status[i] == _abi.OK else _error(status[i], _abi.batch_error(i)) for i in range(n)]
+
+    def decode_device(self, data, frames, alloc, length: Optional[int] = None, stream=None
+                      ) -> List[Union["DeviceFrame", Error]]:
+        """Decodes frames that lie in device memory into device buffers that
+        `alloc(n_samples)` makes (for example torch int16/uint16 tensors on
+        the device); no bitstream or plane crosses to the host."""
+        n_bytes = int(length if length is not None else data.numel())
+        n = len(frames)
+        probes = self.probe_device(data, frames, n_bytes)
+        outs = (Frame_ * max(n, 1))()
+        status = (ctypes.c_int * max(n, 1))()
+        bufs = [None] * n
+        for i, info in enumerate(probes):
+            if isinstance(info, Error):
+                continue
+            d = alloc(info.data_len)
+            a = alloc(info.alpha_len) if info.alpha_len else None
+            bufs[i] = (d, a)
+            outs[i].data = ctypes.cast(_device_ptr(d), ctypes.POINTER(ctypes.c_uint16))
+            outs[i].data_len = info.data_len
+            if a is not None:
+                outs[i].alpha = ctypes.cast(_device_ptr(a), ctypes.POINTER(ctypes.c_uint16))
+                outs[i].alpha_len = info.alpha_len
+        _check(_abi.lib().prores_decode_device(context(self.device).handle, _device_ptr(data), n_bytes,
+                                               _spans(frames), n, self.bit_depth or 0, outs, status,
+                                               _stream_ptr(stream)))
+        res: List[Union[DeviceFrame, Error]] = []
+        for i in range(n):
+            if status[i] != _abi.OK:
+                res.append(_error(status[i], _abi.batch_error(i)))
+                continue
+            f = outs[i]
+            res.append(DeviceFrame(f.width, f.height, f.bit_depth, ChromaFormat(f.chroma), Interlace(f.interlace),
+                                   Metadata(f.aspect_ratio, f.frame_rate_code, f.color_primaries,
+                                            f.transfer_characteristic, f.matrix_coefficients),
+                                   bufs[i][0], bufs[i][1]))
+        return res
+
+
+def scan_frames(data) -> List[tuple]:
+    """The (offset, length) of every whole frame in a MOV file or a prefix of
+    one, found by its 'icpf' identifier and frame_size without parsing the
+    container (the crate's tests/sample.rs:20-38)."""
+    a = _as_u8(data) if len(data) else np.zeros(1, np.uint8)
+    L = _abi.lib()
+    ptr = a.ctypes.data_as(ctypes.c_char_p)
+    n = L.prores_scan_frames(ptr, len(data), None, 0)
+    spans = (_abi.Span_ * max(n, 1))()
+    L.prores_scan_frames(ptr, len(data), spans, n)
+    return [(spans[i].offset, spans[i].len) for i in range(n)]
+
+
+def _device_ptr(x) -> int:
+    return int(x.data_ptr()) if hasattr(x, "data_ptr") else int(x)
+
+
+@dataclass
+class DeviceFrame:
+    """A frame decoded into device memory: the crate's Frame fields, with
+    `data` and `alpha` the caller's device buffers (for example torch
+    tensors) holding Y'‖Cb‖Cr and the alpha plane."""
+
+    width: int
+    height: int
+    bit_depth: int
+    chroma: "ChromaFormat"
+    interlace: "Interlace"
+    metadata: "Metadata"
+    data: object
+    alpha: object = None
+
+
+def _spans(frames) -> "ctypes.Array":
+    arr = (_abi.Span_ * max(len(frames), 1))()
+    for i, (off, n) in enumerate(frames):
+        arr[i].offset, arr[i].len = int(off), int(n)
+    return arr
+
+
+def scan_frames_device(data, length: Optional[int] = None, stream=None, device: int = 0) -> List[tuple]:
+    """scan_frames over bytes in device memory (`data`: a device pointer or
+    an object with data_ptr(), such as a torch uint8 tensor)."""
+    n_bytes = int(length if length is not None else data.numel())
+    ctx = context(device)
+    L = _abi.lib()
+    cap = 1024
+    while True:
+        spans = (_abi.Span_ * cap)()
+        count = ctypes.c_size_t()
+        _check(L.prores_scan_frames_device(ctx.handle, _device_ptr(data), n_bytes, spans, cap, ctypes.byref(count),
+                                           _stream_ptr(stream)))
+        if count.value <= cap:
+            return [(spans[i].offset, spans[i].len) for i in range(count.value)]
+        cap = count.value
 
 
 def replace_decoder(d: Decoder, **kw) -> Decoder:

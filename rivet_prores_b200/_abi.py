@@ -58,6 +58,10 @@ class Buf_(ctypes.Structure):
     _fields_ = [("data", P(ctypes.c_uint8)), ("len", ctypes.c_size_t)]
 
 
+class Span_(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_size_t), ("len", ctypes.c_size_t)]
+
+
 class FrameHeader_(ctypes.Structure):
     _fields_ = [
         ("frame_size", ctypes.c_uint32),
@@ -143,6 +147,13 @@ def lib():
         "prores_job_kernel_times": (ctypes.c_int, [vp, ctypes.c_int, P(ctypes.c_char_p), P(ctypes.c_float),
                                                    ctypes.c_int]),
         "prores_tuning_default": (None, [P(Tuning_)]),
+        "prores_scan_frames": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t, P(Span_), ctypes.c_size_t]),
+        "prores_scan_frames_device": (ctypes.c_int, [vp, vp, ctypes.c_size_t, P(Span_), ctypes.c_size_t,
+                                                     P(ctypes.c_size_t), vp]),
+        "prores_probe_device": (ctypes.c_int, [vp, vp, ctypes.c_size_t, P(Span_), ctypes.c_int, ctypes.c_uint32,
+                                               P(Frame_), P(ctypes.c_int)]),
+        "prores_decode_device": (ctypes.c_int, [vp, vp, ctypes.c_size_t, P(Span_), ctypes.c_int, ctypes.c_uint32,
+                                                P(Frame_), P(ctypes.c_int), vp]),
         "prores_set_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
         "prores_get_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
     }

@@ -224,7 +224,7 @@ __device__ int decode_alpha(Bits &b, const FrameDesc &fd, const PicDesc &pd, con
     const uint32_t ncols = min(cols, width - x0);
     const int32_t mask = (int32_t)((1u << bits) - 1u);
     const uint32_t mag_bits = bits == 8 ? 3u : 6u;
-    uint16_t *plane = alpha + fd.alpha_off;
+    uint16_t *plane = fd.out_alpha ? fd.out_alpha : alpha + fd.alpha_off;
     int32_t prev = -1;
     uint32_t n = 0;
     int err;
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
         const uint32_t per_mb = c == 0 ? 4u : cpm;
         const uint32_t nb = comp_blocks[c];
         const uint32_t pw = fd.plane_w[c];
-        uint16_t *plane = d.planes + fd.plane_off[c];
+        uint16_t *plane = fd.out_planes ? fd.out_planes + (fd.plane_off[c] - fd.plane_off[0]) : d.planes + fd.plane_off[c];
         for (uint32_t t = tid; t < 16u * segs; t += kIdctThreads) {
             const uint32_t r = t / segs, sx = t - r * segs;
             uint32_t m, bb;

@@ -23,6 +23,11 @@ struct FrameDesc {
     uint32_t weights;     // index of this frame's (luma, chroma) weight pair
     uint32_t rescale_identity;
     float out_scale, out_bias, out_max;  // §7.5.1: floor(v scale + bias) in [0, max]
+    // When set (decoding into caller device memory): the frame's packed
+    // planes Y'‖Cb‖Cr (same layout as in the plane buffer) and its alpha
+    // plane go here instead of the workspace's buffers.
+    uint16_t *out_planes;
+    uint16_t *out_alpha;
 };
 
 // One picture (a frame, or one field of an interlaced frame).

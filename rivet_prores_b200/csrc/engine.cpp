@@ -10,6 +10,7 @@
 
 #include "engine.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -259,8 +260,12 @@ static uint32_t add_weights(std::vector<uint8_t> &w, const FrameHeader &h) {
     return (uint32_t)(w.size() / 128 - 1);
 }
 
-Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan) {
+Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan, const FrameBytes *bytes) {
     plan = DecodePlan();
+    plan.device_bits = bytes != nullptr;
+    const auto read = [&](int i, size_t pos, size_t len) -> const uint8_t * {
+        return bytes ? (*bytes)(i, pos, len) : in[i].data + pos;
+    };
     plan.frames.resize(n);
     size_t bits_pos = 0;
     const uint8_t *prev_end = nullptr;
@@ -281,7 +286,12 @@ Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &
             f.err = make_status(PRORES_CONFIG, strf("output bit depth %u is outside 8\xe2\x80\x93" "16", out_depth));
             continue;
         }
-        if ((f.err = parse_frame_header(in[i].data, in[i].len, &f.hdr))) continue;
+        const uint8_t *head = read(i, 0, std::min(in[i].len, kFrameHeadBytes));
+        if (!head) {
+            f.err = make_status(PRORES_DEVICE, "the frame header was not fetched");
+            continue;
+        }
+        if ((f.err = parse_frame_header(head, in[i].len, &f.hdr))) continue;
         if ((f.err = check_plausible_size(f.hdr))) continue;
         const FrameHeader &h = f.hdr;
         f.depth = out_depth ? out_depth : (h.chroma == PRORES_CHROMA_422 ? 10u : 12u);
@@ -327,7 +337,12 @@ Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &
                 break;
             }
             PictureHeader ph;
-            if ((f.late = parse_picture_header(in[i].data + pos, flen - pos, &ph))) break;
+            const uint8_t *pic = read(i, pos, std::min(flen - pos, (size_t)kPictureHeaderSize));
+            if (!pic) {
+                f.late = make_status(PRORES_DEVICE, "a picture header was not fetched");
+                break;
+            }
+            if ((f.late = parse_picture_header(pic, flen - pos, &ph))) break;
             const uint32_t height = h.picture_height(index);
             const uint32_t height_in_mb = (height + 15u) / 16u;
             const uint32_t spr = slices_per_row(width_in_mb, ph.log2_slice_mbs);
@@ -365,7 +380,9 @@ Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &
 Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s) {
     (void)in;
     for (const auto &c : plan.copies)
-        PR_CUDA(ws.stager.h2d(ws.bits.as<uint8_t>() + c.dst, c.src, c.len, s),
+        PR_CUDA(plan.device_bits ? cudaMemcpyAsync(ws.bits.as<uint8_t>() + c.dst, c.src, c.len,
+                                                   cudaMemcpyDeviceToDevice, s)
+                                 : ws.stager.h2d(ws.bits.as<uint8_t>() + c.dst, c.src, c.len, s),
                 "bitstream upload");
     return Status();
 }
@@ -441,7 +458,7 @@ Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaS
 }
 
 Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
-                    Status *first_err) {
+                    Status *first_err, bool device_out) {
     const size_t n_pics = plan.pdesc.size();
     PR_CUDA(ws.host_small.reserve(sizeof(PicStatus) * (n_pics + 1)), "cudaMallocHost");
     PicStatus *ps_host = static_cast<PicStatus *>(ws.host_small.p);
@@ -457,7 +474,7 @@ Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prore
     };
     std::vector<Run> runs;
     const int n = (int)plan.frames.size();
-    for (int i = 0; i < n; i++) {
+    for (int i = 0; i < n && !device_out; i++) {
         const DecodeFrame &f = plan.frames[i];
         prores_frame &o = out[i];
         if (f.err) continue;
@@ -559,6 +576,35 @@ static bool profiling_requested() {
     return v && v[0] && v[0] != '0';
 }
 
+namespace prores {
+
+Status probe_frame(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info) {
+    if (out_bit_depth != 0 && (out_bit_depth < 8 || out_bit_depth > 16))
+        return (make_status(PRORES_CONFIG, strf("output bit depth %u is outside 8\xe2\x80\x93" "16", out_bit_depth)));
+    FrameHeader h;
+    Status st = parse_frame_header(data, len, &h);
+    if (!st) st = check_plausible_size(h);
+    if (st) return st;
+    memset(info, 0, sizeof *info);
+    info->width = h.width;
+    info->height = h.height;
+    info->bit_depth = out_bit_depth ? out_bit_depth : (h.chroma == PRORES_CHROMA_422 ? 10u : 12u);
+    info->chroma = h.chroma;
+    info->interlace = h.interlace;
+    info->aspect_ratio = h.aspect_ratio;
+    info->frame_rate_code = h.frame_rate_code;
+    info->color_primaries = h.color_primaries;
+    info->transfer_characteristic = h.transfer_characteristic;
+    info->matrix_coefficients = h.matrix_coefficients;
+    size_t off[3];
+    uint32_t w[3];
+    info->data_len = frame_layout(h.width, h.height, h.chroma, off, w);
+    info->alpha_len = h.alpha ? (size_t)h.width * h.height : 0;
+    return Status();
+}
+
+}  // namespace prores
+
 extern "C" {
 
 prores_ctx *prores_create(int device) {
@@ -641,28 +687,7 @@ const char *prores_batch_error(int i) {
 }
 
 int prores_probe(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info) {
-    if (out_bit_depth != 0 && (out_bit_depth < 8 || out_bit_depth > 16))
-        return fail(make_status(PRORES_CONFIG, strf("output bit depth %u is outside 8\xe2\x80\x93" "16", out_bit_depth)));
-    FrameHeader h;
-    Status st = parse_frame_header(data, len, &h);
-    if (!st) st = check_plausible_size(h);
-    if (st) return fail(st);
-    memset(info, 0, sizeof *info);
-    info->width = h.width;
-    info->height = h.height;
-    info->bit_depth = out_bit_depth ? out_bit_depth : (h.chroma == PRORES_CHROMA_422 ? 10u : 12u);
-    info->chroma = h.chroma;
-    info->interlace = h.interlace;
-    info->aspect_ratio = h.aspect_ratio;
-    info->frame_rate_code = h.frame_rate_code;
-    info->color_primaries = h.color_primaries;
-    info->transfer_characteristic = h.transfer_characteristic;
-    info->matrix_coefficients = h.matrix_coefficients;
-    size_t off[3];
-    uint32_t w[3];
-    info->data_len = frame_layout(h.width, h.height, h.chroma, off, w);
-    info->alpha_len = h.alpha ? (size_t)h.width * h.height : 0;
-    return PRORES_OK;
+    return fail_or_ok(probe_frame(data, len, out_bit_depth, info));
 }
 
 int prores_parse_frame_header(const uint8_t *data, size_t len, prores_frame_header *out) {

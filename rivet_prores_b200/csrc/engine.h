@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -138,15 +139,24 @@ struct DecodePlan {
         size_t dst, len;
     };
     std::vector<Copy> copies;
+    bool device_bits = false;  // the frames lie in device memory: copies are device to device
 };
 
-Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan);
+// Where plan_decode reads the frames' header bytes: read(i, pos, len) gives
+// a host pointer to bytes [pos, pos + len) of frame i, or null when they are
+// not at hand. Without it, the frames themselves are host memory.
+using FrameBytes = std::function<const uint8_t *(int frame, size_t pos, size_t len)>;
+// The bytes of the frame header that planning reads (8 + 20 + two 64-byte
+// matrices, rounded up).
+constexpr size_t kFrameHeadBytes = 160;
+Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &plan,
+                   const FrameBytes *bytes = nullptr);
 Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s);
 Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s);
 DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan &plan);
 Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s, KernelTimes *kt);
 Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
-                    Status *first_err);
+                    Status *first_err, bool device_out = false);
 
 // ---- encode
 
@@ -165,6 +175,8 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
                     int *status, Status *first_err);
 
 void set_last_error(const Status &s);
+// prores_probe's work: the frame header, checked, as sizes and metadata.
+Status probe_frame(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info);
 // Per-frame messages of the last batch call on this thread.
 void set_batch_errors(const std::vector<Status> &errs);
 Status record_kernel(KernelTimes *kt, const char *name, cudaStream_t s);
