@@ -209,6 +209,15 @@ int prores_probe_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len,
 int prores_decode_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len, const prores_span *frames, int n,
                          uint32_t out_bit_depth, prores_frame *out, int *status, void *stream);
 
+/* Encoder::encode (src/encode.rs:223-287) for n frames whose planes (and
+ * alpha) lie in device memory: in[i].data and in[i].alpha are device
+ * pointers, everything else as in prores_encode_batch, whose packets (host,
+ * library-allocated) and statuses this returns. The planes are copied
+ * device to device; the work runs on `stream` (a cudaStream_t, or NULL)
+ * and the call returns when it is done. */
+int prores_encode_device(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n, prores_buf *out,
+                         int *status, void *stream);
+
 /* ---- decode without device allocation --------------------------------- */
 
 /* Size of the fixed device array prores_decode_noalloc keeps its scratch in:

@@ -663,6 +663,44 @@ class Encoder:
                 L.prores_buffer_free(outs[i].data)
         return res
 
+    def encode_device(self, frames: Sequence["DeviceFrame"], configs: Optional[Sequence[Config]] = None,
+                      stream=None) -> List[Union[bytes, Error]]:
+        """encode_batch for frames whose planes lie in device memory
+        (DeviceFrame: `data`, `alpha` device buffers with data_ptr() and
+        numel(), such as torch tensors); the packets come back to the host."""
+        L = _abi.lib()
+        n = len(frames)
+        configs = list(configs) if configs is not None else [self._config] * n
+        cfgs = (Config_ * max(n, 1))()
+        ins = (Frame_ * max(n, 1))()
+        outs = (Buf_ * max(n, 1))()
+        status = (ctypes.c_int * max(n, 1))()
+        for i, f in enumerate(frames):
+            cfgs[i] = configs[i]._c()
+            c = ins[i]
+            c.width, c.height, c.bit_depth = f.width, f.height, f.bit_depth
+            c.chroma, c.interlace = f.chroma.value, f.interlace.value
+            m = f.metadata
+            (c.aspect_ratio, c.frame_rate_code, c.color_primaries, c.transfer_characteristic,
+             c.matrix_coefficients) = (m.aspect_ratio, m.frame_rate_code, m.color_primaries,
+                                       m.transfer_characteristic, m.matrix_coefficients)
+            c.data = ctypes.cast(_device_ptr(f.data), ctypes.POINTER(ctypes.c_uint16))
+            c.data_len = int(f.data.numel())
+            if f.alpha is not None:
+                c.alpha = ctypes.cast(_device_ptr(f.alpha), ctypes.POINTER(ctypes.c_uint16))
+                c.alpha_len = int(f.alpha.numel())
+        code = L.prores_encode_device(context(self.device).handle, cfgs, ins, n, outs, status, _stream_ptr(stream))
+        if code != _abi.OK:
+            raise _error(code)
+        res: List[Union[bytes, Error]] = []
+        for i in range(n):
+            if status[i] != _abi.OK:
+                res.append(_error(status[i], _abi.batch_error(i)))
+            else:
+                res.append(ctypes.string_at(outs[i].data, outs[i].len))
+                L.prores_buffer_free(outs[i].data)
+        return res
+
 
 # ------------------------------------------------------------------ resident jobs
 

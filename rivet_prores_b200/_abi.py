@@ -154,6 +154,8 @@ def lib():
                                                P(Frame_), P(ctypes.c_int)]),
         "prores_decode_device": (ctypes.c_int, [vp, vp, ctypes.c_size_t, P(Span_), ctypes.c_int, ctypes.c_uint32,
                                                 P(Frame_), P(ctypes.c_int), vp]),
+        "prores_encode_device": (ctypes.c_int, [vp, P(Config_), P(Frame_), ctypes.c_int, P(Buf_), P(ctypes.c_int),
+                                                vp]),
         "prores_set_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
         "prores_get_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
     }

@@ -327,7 +327,8 @@ static size_t cost_bytes(const EncodePlan &plan) {
            4 * kWindow + 256;
 }
 
-static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s) {
+static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s,
+                            bool device_frames) {
     // One copy per host-adjacent run of planes.
     struct Run {
         const uint8_t *src;
@@ -348,16 +349,21 @@ static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_
         add(planes, in[i].data, 2 * fd.in_off[0], 2 * ef.samples);
         if (ef.alpha_samples) add(alpha, in[i].alpha, 2 * fd.alpha_in_off, 2 * ef.alpha_samples);
     }
+    // Frames in device memory are copied device to device.
+    const auto copy = [&](uint8_t *dst, const uint8_t *src, size_t len) {
+        return device_frames ? cudaMemcpyAsync(dst, src, len, cudaMemcpyDeviceToDevice, s)
+                             : ws.stager.h2d(dst, src, len, s);
+    };
     for (const Run &r : planes)
-        PR_CUDA(ws.stager.h2d(ws.enc_in.as<uint8_t>() + r.dst, r.src, r.len, s), "frame upload");
+        PR_CUDA(copy(ws.enc_in.as<uint8_t>() + r.dst, r.src, r.len), "frame upload");
     for (const Run &r : alpha)
-        PR_CUDA(ws.stager.h2d(ws.enc_alpha_in.as<uint8_t>() + r.dst, r.src, r.len, s),
+        PR_CUDA(copy(ws.enc_alpha_in.as<uint8_t>() + r.dst, r.src, r.len),
                 "alpha upload");
     return Status();
 }
 
 Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores_frame *in, cudaStream_t s,
-                     bool descriptors) {
+                     bool descriptors, bool device_frames) {
     (void)ctx;
     if (descriptors) {
         PR_CUDA(ws.enc_in.reserve(2 * (plan.in_total + 8)), "cudaMalloc frames");
@@ -390,7 +396,7 @@ Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores
             PR_CUDA(ws.stager.h2d(ws.enc_frame_out.p, plan.headers.data(), plan.headers.size(), s),
                     "upload");
     }
-    return upload_frames(ws, plan, in, s);
+    return upload_frames(ws, plan, in, s, device_frames);
 }
 
 static Status enqueue_tail(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, KernelTimes *kt) {
@@ -518,8 +524,8 @@ static bool profiling_on() {
 
 extern "C" {
 
-int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n, prores_buf *out,
-                        int *status) {
+static int encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n, prores_buf *out,
+                        int *status, bool device_frames, void *stream) {
     if (!ctx || n < 0) return efail(make_status(PRORES_CONFIG, "no context"));
     cudaSetDevice(ctx->impl.device);
     EncodePlanPtr plan;
@@ -527,8 +533,8 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
     if (st) return efail(st);
     auto ws = ctx->impl.acquire();
     if (!ws) return efail(make_status(PRORES_DEVICE, "no stream"));
-    cudaStream_t s = ws->stream;
-    st = upload_encode(ctx->impl, *ws, *plan, in, s, true);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    st = upload_encode(ctx->impl, *ws, *plan, in, s, true, device_frames);
     if (!st) st = enqueue_encode(ctx->impl, *ws, *plan, s, nullptr);
     std::vector<prores_buf> packets;
     Status first;
@@ -562,6 +568,16 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
     return PRORES_OK;
 }
 
+int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n, prores_buf *out,
+                        int *status) {
+    return encode_batch(ctx, cfg, in, n, out, status, false, nullptr);
+}
+
+int prores_encode_device(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, int n, prores_buf *out,
+                         int *status, void *stream) {
+    return encode_batch(ctx, cfg, in, n, out, status, true, stream);
+}
+
 int prores_encode(prores_ctx *ctx, const prores_config *cfg, const prores_frame *in, uint8_t **out, size_t *out_len) {
     prores_buf b{nullptr, 0};
     int status = PRORES_OK;
@@ -584,7 +600,7 @@ int prores_encode_job_create(prores_ctx *ctx, const prores_config *cfg, const pr
         j->ws = ctx->impl.acquire();
         if (!j->ws) st = make_status(PRORES_DEVICE, "no stream");
     }
-    if (!st) st = upload_encode(ctx->impl, *j->ws, *j->plan, in, j->ws->stream, true);
+    if (!st) st = upload_encode(ctx->impl, *j->ws, *j->plan, in, j->ws->stream, true, false);
     if (!st) st = cuda_status(cudaStreamSynchronize(j->ws->stream), "upload");
     if (st) {
         prores_encode_job_destroy(j);
@@ -605,7 +621,7 @@ int prores_encode_job_upload(prores_encode_job *job, const prores_frame *in, int
     }
     cudaSetDevice(job->ctx->impl.device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
-    Status st = upload_encode(job->ctx->impl, *job->ws, *job->plan, in, s, false);
+    Status st = upload_encode(job->ctx->impl, *job->ws, *job->plan, in, s, false, false);
     return st ? efail(st) : PRORES_OK;
 }
 

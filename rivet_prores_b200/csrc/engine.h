@@ -167,7 +167,7 @@ struct EncodePlanDeleter {
 using EncodePlanPtr = std::unique_ptr<EncodePlan, EncodePlanDeleter>;
 Status plan_encode(const prores_config *cfg, const prores_frame *in, int n, EncodePlanPtr &plan);
 Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores_frame *in, cudaStream_t s,
-                     bool descriptors);
+                     bool descriptors, bool device_frames = false);
 Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t s, KernelTimes *kt);
 // Waits for the encode and stages the packets in the workspace's pinned
 // buffer; out[i] points into it until the workspace's next fetch.

@@ -62,3 +62,22 @@ def test_spans_outside_the_buffer_are_refused():
     d = _to_device(b"\0" * 100)
     with pytest.raises(P.Error.Config):
         P.Decoder.new().decode_device(d, [(90, 20)], lambda k: None)
+
+
+def test_encode_from_device_memory_equals_the_host_encode():
+    """A transcoder's path on the GPU: frames decoded into device memory
+    are encoded from there, and the packets equal the host path's."""
+    import torch
+
+    data, spans = mov_like(4)
+    d = _to_device(data)
+    alloc = lambda k: torch.empty(k, dtype=torch.int16, device="cuda")  # noqa: E731
+    dev_frames = P.Decoder.new().decode_device(d, spans, alloc)
+    host_frames = P.Decoder.new().decode_batch([data[o:o + k] for o, k in spans])
+    configs = [P.Config(P.Profile.P4444 if f.chroma == P.ChromaFormat.Yuv444 else P.Profile.Hq, log2_slice_mbs=i % 4)
+               for i, f in enumerate(host_frames)]
+    enc = P.Encoder(configs[0])
+    for rep in range(2):
+        got = enc.encode_device(dev_frames, configs)
+        want = enc.encode_batch(host_frames, configs)
+        assert got == want
