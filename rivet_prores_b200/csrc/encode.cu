@@ -928,25 +928,65 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
         // The next chunk's thresholds, fetched while this chunk is walked.
         if (k + 32 < pd.n_slices) next = e.share_prep[pd.slice_base + k + 32];
         uint32_t my_steps = 0;
-        uint32_t done = 0;
+        uint32_t done = 0;  // lanes below are settled
         while (done < 32u) {
-            bool deep;
-            const uint32_t ks = live ? steps_at(mine, D, st.uniform, deep) : 0u;
-            const bool stepping = live && lane >= (int)done && (ks > 0 || deep);
-            const uint32_t mask = __ballot_sync(0xffffffffu, stepping);
-            if (!mask) break;
-            const uint32_t f = __ffs(mask) - 1;
+            // The walk is sequential: a slice's slack D is what the slices
+            // before it left. Each lane guesses its D, takes its steps there,
+            // and the guesses are redone from the exclusive sum of the steps'
+            // size changes until none moves. A lane's D depends only on the
+            // lanes before it, so after t rounds the first t lanes are exact
+            // and the fixed point reached (at most 33 rounds) is the
+            // sequential walk's. Lanes from the first one that needs a level
+            // nobody costed (`deep`) on wait for the warp to cost it.
+            uint64_t myD = D;
+            uint32_t ks = 0;
+            int64_t dl = 0;
+            uint32_t first_deep = 32;
+            for (int round = 0; round < 34; round++) {
+                bool deep = false;
+                ks = live && (uint32_t)lane >= done ? steps_at(mine, myD, st.uniform, deep) : 0u;
+                const uint32_t deep_mask = __ballot_sync(0xffffffffu, live && (uint32_t)lane >= done && deep);
+                const uint32_t fd_lane = deep_mask ? (uint32_t)__ffs(deep_mask) - 1u : 32u;
+                int64_t mine_dl = 0;
+#pragma unroll
+                for (int j = 0; j < kWindow; j++)
+                    if ((uint32_t)j + 1u == ks) mine_dl = mine.delta[j];
+                dl = (uint32_t)lane < fd_lane ? mine_dl : 0;
+                // Inclusive sum of dl over the lanes.
+                int64_t incl = dl;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int64_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const uint64_t newD = (uint64_t)((int64_t)D - (incl - dl));
+                const bool moved = (uint32_t)lane >= done && (uint32_t)lane <= fd_lane && newD != myD;
+                myD = newD;
+                const bool again = __any_sync(0xffffffffu, moved) || fd_lane != first_deep;
+                first_deep = fd_lane;
+                if (!again) break;
+            }
+            // Lanes done .. first_deep - 1 are settled at myD with ks steps.
+            if ((uint32_t)lane >= done && (uint32_t)lane < first_deep) my_steps = ks;
+            const int64_t settled = __shfl_sync(0xffffffffu, (int64_t)D - (int64_t)myD, first_deep < 32u ? first_deep : 31u);
+            if (first_deep >= 32u) {
+                // Every lane settled: D after the chunk.
+                const int64_t total = __shfl_sync(0xffffffffu, (int64_t)D - (int64_t)myD + dl, 31);
+                D = (uint64_t)((int64_t)D - total);
+                break;
+            }
+            // The deep lane, at its exact D: the warp costs quantiser qi - 1
+            // and the slice steps while it fits its allowance (fixed during
+            // the slice's walk).
+            D = (uint64_t)((int64_t)D - settled);
+            const uint32_t f = first_deep;
             const uint32_t fk = __shfl_sync(0xffffffffu, ks, f);
-            const bool fdeep = __shfl_sync(0xffffffffu, deep, f);
             int64_t delta = fk ? (int64_t)__shfl_sync(0xffffffffu, mine.delta[0], f) : 0;
 #pragma unroll
             for (int j = 1; j < kWindow; j++)
                 if ((uint32_t)j == fk - 1) delta = __shfl_sync(0xffffffffu, mine.delta[j], f);
             uint32_t steps = fk;
-            if (fdeep) {
-                // Past the window: the warp costs quantiser qi - 1 and the
-                // slice steps while it fits its allowance (fixed during the
-                // slice's walk).
+            {
                 const uint32_t s = pd.slice_base + k0 + f;
                 const EncSliceDesc fsd = e.slices[s];
                 const uint32_t fbase = __shfl_sync(0xffffffffu, mine.base, f);
