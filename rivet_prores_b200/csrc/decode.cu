@@ -29,6 +29,7 @@
 namespace prores {
 
 __constant__ uint8_t c_scan[2][64];
+__constant__ float c_idct_basis[64];  // T[x][u] (dct_basis)
 
 namespace {
 
@@ -496,13 +497,12 @@ __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_
     }
 }
 
-__global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
+__global__ void __launch_bounds__(kIdctThreads, 4) k_idct(DecodeLaunch d) {
     extern __shared__ __align__(16) unsigned char smem[];
     int32_t *cs = reinterpret_cast<int32_t *>(smem);                   // scanned coefficients
     float *tmp = reinterpret_cast<float *>(smem + 4 * kMaxSliceCoefs);  // row pass, [v][x][blk] per component
     uint8_t *nz = smem + 8 * kMaxSliceCoefs;                           // non-zero rows, [blk][v]
     __shared__ float scale[2][64];
-    __shared__ float basis[64];
     __shared__ uint8_t scan[64];
 
     const SliceDesc sd = d.slices[blockIdx.x];
@@ -538,9 +538,7 @@ __global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
         // F = QF * (W * qScale / 8), one factor per raster position (src/decode.rs:356).
         scale[which][k] = (float)((uint32_t)d.weights[fd.weights * 128u + which * 64u + k] * q) / 8.0f;
     } else if (tid < 192) {
-        basis[tid - 128] = d.tables.basis[tid - 128];
-    } else {
-        scan[tid - 192] = c_scan[pd.interlaced_scan][tid - 192];
+        scan[tid - 128] = c_scan[pd.interlaced_scan][tid - 128];
     }
     __syncthreads();
 
@@ -576,7 +574,7 @@ __global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
             for (int x = 0; x < 8; x++) {
                 float s = 0.0f;
 #pragma unroll
-                for (int u = 0; u < 8; u++) s = __fadd_rn(s, __fmul_rn(row[u], basis[8 * x + u]));
+                for (int u = 0; u < 8; u++) s = __fadd_rn(s, __fmul_rn(row[u], c_idct_basis[8 * x + u]));
                 dst[(v * 8u + x) * nb + blk] = s;
             }
         }
@@ -619,7 +617,7 @@ __global__ void __launch_bounds__(kIdctThreads, 3) k_idct(DecodeLaunch d) {
 #pragma unroll
             for (int v = 0; v < 8; v++) {
                 if (!nz[gblk * 8u + v]) continue;
-                const float w = basis[8u * y + v];
+                const float w = c_idct_basis[8u * y + v];
 #pragma unroll
                 for (int x = 0; x < 8; x++) acc[x] = __fadd_rn(acc[x], __fmul_rn(w, src[(v * 8u + x) * nb + blk]));
             }
@@ -711,6 +709,9 @@ cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s) {
 cudaError_t configure_decode_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_idct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)idct_smem_bytes());
     if (e != cudaSuccess) return e;
+    float basis[64];
+    dct_basis(basis);
+    if ((e = cudaMemcpyToSymbol(c_idct_basis, basis, sizeof basis)) != cudaSuccess) return e;
     return upload_scans();
 }
 
