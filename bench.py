@@ -42,11 +42,11 @@ ALGO_BYTES_PER_FRAME = 3_643_238 + 2 * (W * H * 2)
 # traffic grows with the frames a launch covers). k_cost is the mean of its
 # nine probe launches.
 PROFILED = {
-    "k_cost": {"dram_bytes_per_frame": 51.41e6, "issue_active_pct": "52-71"},
-    "k_idct": {"dram_bytes_per_frame": 73.19e6, "issue_active_pct": "59"},
-    "k_fdct": {"dram_bytes_per_frame": 97.87e6, "issue_active_pct": "38"},
-    "k_entropy": {"dram_bytes_per_frame": 70.97e6, "issue_active_pct": "46"},
-    "k_pack": {"dram_bytes_per_frame": 78.98e6, "issue_active_pct": "72"},
+    "k_cost": {"dram_bytes_per_frame": 51.37e6, "issue_active_pct": "52-71"},
+    "k_idct": {"dram_bytes_per_frame": 73.01e6, "issue_active_pct": "66"},
+    "k_fdct": {"dram_bytes_per_frame": 97.76e6, "issue_active_pct": "83"},
+    "k_entropy": {"dram_bytes_per_frame": 71.34e6, "issue_active_pct": "44"},
+    "k_pack": {"dram_bytes_per_frame": 78.86e6, "issue_active_pct": "72"},
 }
 
 
