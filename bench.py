@@ -437,7 +437,7 @@ def run_serving(args, device):
                            "pooled page-locked buffers"}
     # Batches of at most 16: large enough to fill the device, small enough
     # that a request does not wait behind a long batch.
-    for name, workers, max_batch, seconds in [("batched", 3, 16, args.serve_seconds),
+    for name, workers, max_batch, seconds in [("batched", 4, 16, args.serve_seconds),
                                               ("plain", 1, 1, max(1.0, args.serve_seconds / 4))]:
         # One backend (and its pool of page-locked output buffers) for the
         # warm-up and the measured run.

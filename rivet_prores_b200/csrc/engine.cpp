@@ -57,10 +57,12 @@ static size_t grown(size_t bytes, size_t cap) {
 cudaError_t DeviceBuf::reserve(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     const size_t want = grown(bytes, cap);
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, stream);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, stream);
+    // Usable from any stream once the workspace's stream has passed it.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) {
         p = nullptr;
         return e;
@@ -174,6 +176,13 @@ cudaError_t Stager::finish() {
     return cudaSuccess;
 }
 
+void Workspace::bind_stream() {
+    for (DeviceBuf *b : {&bits, &frames, &pics, &slices, &slot_status, &pic_status, &coef, &coef_count, &planes,
+                         &alpha, &weights, &counter, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost, &enc_pic_state,
+                         &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes, &enc_frame_out})
+        b->stream = stream;
+}
+
 Workspace::~Workspace() {
     if (stream) cudaStreamDestroy(stream);
 }
@@ -191,6 +200,7 @@ std::unique_ptr<Workspace> Context::acquire() {
     ws->device = device;
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    ws->bind_stream();
     return ws;
 }
 
@@ -632,6 +642,14 @@ prores_ctx *prores_create(int device) {
         fail(st);
         delete ctx;
         return nullptr;
+    }
+    // Workspace buffers are allocated stream-ordered from the device's
+    // default pool; keep up to 8 GiB of freed memory in it for the next
+    // growth instead of handing it back at every synchronisation.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = 8ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     ctx->impl.entropy = EntropyShape{ctx->impl.tuning.entropy_warps_per_block,
                                      entropy_grid(device, ctx->impl.tuning.entropy_warps_per_block,

@@ -17,9 +17,14 @@
 namespace prores {
 
 // A device allocation that only grows.
+// A device buffer that grows on demand. It is allocated stream-ordered on
+// its workspace's stream (set when the workspace is made), and the growth
+// waits for that stream only: cudaFree and cudaMalloc would wait for the
+// whole device, which stalls every other thread's batch.
 struct DeviceBuf {
     void *p = nullptr;
     size_t cap = 0;
+    cudaStream_t stream = nullptr;
     cudaError_t reserve(size_t bytes);
     template <class T>
     T *as() const {
@@ -71,6 +76,8 @@ struct Workspace {
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
     PinnedBuf host_stage;
+    // Points every DeviceBuf at the workspace's stream.
+    void bind_stream();
     // Statuses and sizes read back each call. Pinned, because a copy into
     // pageable memory returns only when done and keeps other host threads'
     // CUDA calls waiting meanwhile.
