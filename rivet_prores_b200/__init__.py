@@ -345,7 +345,7 @@ class Tuning:
     """Launch shapes and host pipeline depth (prores_tuning in the C ABI).
     None of them changes an output; `autotune` picks them per GPU."""
 
-    cost_lane_items_per_sm: int = 1024
+    cost_lane_items_per_sm: int = 640
     entropy_warps_per_block: int = 8
     entropy_blocks_per_sm: int = 0
     entropy_components_per_lane: int = 1

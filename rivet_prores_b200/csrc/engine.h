@@ -95,7 +95,7 @@ struct KernelTimes {
 
 // Launch shapes and pipeline depth (prores_tuning); none changes any output.
 struct Tuning {
-    int cost_lane_items_per_sm = 1024;
+    int cost_lane_items_per_sm = 640;  // the autotuner's choice on a B200: lanes from 8 UHD frames up
     int entropy_warps_per_block = 8;
     int entropy_blocks_per_sm = 0;
     int entropy_components_per_lane = 1;
