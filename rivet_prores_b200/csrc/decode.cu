@@ -132,19 +132,46 @@ __device__ __forceinline__ int read_sym(Bits &b, const uint16_t *tab, Codebook c
     return DE_OK;
 }
 
-__device__ __forceinline__ uint64_t entry(uint32_t n, int32_t v) { return ((uint64_t)n << 32) | (uint32_t)v; }
+// A component's coefficient list, in a region of 2 cap 32-bit words (cap =
+// 64 n_blocks, the component's positions): entries from the front, each
+// (scanned index << 21) | value in 21-bit two's complement. Values outside
+// [kListMin, 2^20) go to the back of the region, the k-th at 2 cap - 1 - k,
+// and their entry holds -2^20 + k. Half the bytes of (index, value) pairs
+// of 32-bit words, for values of any size.
+constexpr int32_t kListMin = -(1 << 20) + 2048;
+
+struct CoefList {
+    uint32_t *w;
+    uint32_t cap, big;
+    __device__ __forceinline__ void put(uint32_t &count, uint32_t n, int32_t v) {
+        if (v >= kListMin && v < (1 << 20)) {
+            w[count++] = (n << 21) | ((uint32_t)v & 0x1FFFFFu);
+        } else {
+            w[2u * cap - 1u - big] = (uint32_t)v;
+            w[count++] = (n << 21) | ((uint32_t)(-(1 << 20) + (int32_t)big) & 0x1FFFFFu);
+            big++;
+        }
+    }
+};
+
+// An entry's (index, value), reading a large value from the region's back.
+__device__ __forceinline__ void list_entry(const uint32_t *w, uint32_t cap, uint32_t e, uint32_t &n, int32_t &v) {
+    n = e >> 21;
+    v = (int32_t)(e << 11) >> 11;
+    if (v < kListMin) v = (int32_t)__ldg(w + 2u * cap - 1u - (uint32_t)(v + (1 << 20)));
+}
 
 // scanned_coefficients() of one component (src/decode.rs:484-540): every
 // coefficient the codes give, as (scanned index, value) entries in index
 // order; `count` gets how many (also when decoding fails part-way).
-__device__ int decode_component(Bits &b, uint32_t n_blocks, uint64_t *out, uint32_t &count, const uint16_t *run_tab,
+__device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32_t &count, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
     count = 0;
     uint32_t sym;
     int err = read_sym(b, nullptr, kFirstDcBook, sym);
     if (err) return err;
     int32_t prev_dc = symbol_to_signed(sym);
-    out[count++] = entry(0, prev_dc);
+    out.put(count, 0, prev_dc);
     int32_t prev_diff = 3;
     for (uint32_t i = 1; i < n_blocks; i++) {
         if ((err = read_sym(b, nullptr, dc_book(prev_diff), sym))) return err;
@@ -153,7 +180,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, uint64_t *out, uint3
         int64_t s = (int64_t)prev_dc + diff;
         if (s > INT32_MAX || s < INT32_MIN) return DE_DC_OVERFLOW;
         prev_dc = (int32_t)s;
-        out[count++] = entry(i, prev_dc);
+        out.put(count, i, prev_dc);
         prev_diff = diff;
     }
     const uint32_t total = n_blocks * 64;
@@ -178,7 +205,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, uint64_t *out, uint3
                     int32_t level = (int32_t)lvl + 1;
                     bool neg = (w2 << l2) >> 63;
                     b.pos += l1 + l2 + 1;
-                    out[count++] = entry(n, neg ? -level : level);
+                    out.put(count, n, neg ? -level : level);
                     n += 1;
                     prev_run = run;
                     prev_level = lvl;
@@ -203,7 +230,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, uint64_t *out, uint3
         bool neg = b.peek() >> 63;
         b.pos += 1;
         int32_t level = (int32_t)lvl + 1;
-        out[count++] = entry(n, neg ? -level : level);
+        out.put(count, n, neg ? -level : level);
         n += 1;
     }
     return DE_OK;
@@ -345,7 +372,8 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
         const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
         const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
         uint32_t count = 0;
-        err = decode_component(b, n_blocks, d.coef + base, count, run_tab, level_tab);
+        const CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u};
+        err = decode_component(b, n_blocks, list, count, run_tab, level_tab);
         d.coef_count[3ull * s + comp] = count;
     }
     *slot = make_int2(err, 0);
@@ -523,11 +551,12 @@ __global__ void __launch_bounds__(kIdctThreads, 4) k_idct(DecodeLaunch d) {
         const uint32_t cap = 64u * (c == 0 ? 4u : cpm) * mbs;
         const uint32_t start = c == 0 ? 0u : 64u * mbs * (4u + (c - 1u) * cpm);
         const uint32_t n = min(d.coef_count[3ull * blockIdx.x + c], cap);
-        const uint64_t *list = d.coef + sd.coef + start;
+        const uint32_t *list = reinterpret_cast<const uint32_t *>(d.coef + sd.coef + start);
         for (uint32_t i = tid; i < n; i += kIdctThreads) {
-            const uint64_t e = __ldg(reinterpret_cast<const unsigned long long *>(list) + i);
-            const uint32_t pos = (uint32_t)(e >> 32);
-            if (pos < cap) cs[start + pos] = (int32_t)(uint32_t)e;
+            uint32_t pos;
+            int32_t v;
+            list_entry(list, cap, __ldg(list + i), pos, v);
+            if (pos < cap) cs[start + pos] = v;
         }
     }
     uint32_t qi = sd.size >= 2 ? d.bits[sd.off + 1] : 1u;

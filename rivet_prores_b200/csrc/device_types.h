@@ -91,9 +91,11 @@ struct DecodeLaunch {
     SliceDesc *slices;
     int2 *slot_status;  // 4 per slice
     PicStatus *pic_status;
-    // Decoded coefficients, per slice component: (scanned position << 32 |
-    // value) in position order, in a region as long as the component has
-    // coefficients; coef_count[3 s + c] says how many are there.
+    // Decoded coefficients, per slice component: a list of 32-bit entries
+    // (scanned position << 21 | 21-bit value; larger values at the region's
+    // back, see CoefList in decode.cu) in position order, in a region of
+    // 8 bytes per position of the component; coef_count[3 s + c] says how
+    // many entries there are.
     uint64_t *coef;
     uint32_t *coef_count;
     uint16_t *planes;
