@@ -525,11 +525,11 @@ __device__ __forceinline__ void block_xy(uint32_t comp, uint32_t chroma, uint32_
     }
 }
 
-__global__ void __launch_bounds__(kIdctThreads, 4) k_idct(DecodeLaunch d) {
+__global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
     extern __shared__ __align__(16) unsigned char smem[];
     int32_t *cs = reinterpret_cast<int32_t *>(smem);                   // scanned coefficients
-    float *tmp = reinterpret_cast<float *>(smem + 4 * kMaxSliceCoefs);  // row pass, [v][x][blk] per component
-    uint8_t *nz = smem + 8 * kMaxSliceCoefs;                           // non-zero rows, [blk][v]
+    float *tmp = reinterpret_cast<float *>(smem);  // row pass, over cs: [v][x][blk] per component
+    uint8_t *nz = smem + 4 * kMaxSliceCoefs;       // non-zero rows, [blk][v]
     __shared__ float scale[2][64];
     __shared__ uint8_t scan[64];
 
@@ -580,7 +580,17 @@ __global__ void __launch_bounds__(kIdctThreads, 4) k_idct(DecodeLaunch d) {
     comp_start[1] = 64u * comp_blocks[0];
     comp_start[2] = comp_start[1] + 64u * comp_blocks[1];
     const uint32_t all_blocks = comp_blocks[0] + 2u * comp_blocks[1];
-    for (uint32_t t = tid; t < all_blocks * 8u; t += kIdctThreads) {
+    // The row results are held in registers until every thread has read
+    // its coefficients, then written over them (the two arrays share the
+    // shared memory, so that five CTAs fit on an SM).
+    constexpr int kRowsPerThread = (kMaxSliceCoefs / 8 + kIdctThreads - 1) / kIdctThreads;
+    float held[kRowsPerThread][8];
+    bool held_any[kRowsPerThread];
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; k++) {
+        const uint32_t t = tid + (uint32_t)k * kIdctThreads;
+        held_any[k] = false;
+        if (t >= all_blocks * 8u) continue;
         const uint32_t c = t < comp_blocks[0] * 8u ? 0u : (t < (comp_blocks[0] + comp_blocks[1]) * 8u ? 1u : 2u);
         const uint32_t tc = t - (c == 0 ? 0u : (c == 1 ? comp_blocks[0] * 8u : (comp_blocks[0] + comp_blocks[1]) * 8u));
         const uint32_t nb = comp_blocks[c];
@@ -591,21 +601,35 @@ __global__ void __launch_bounds__(kIdctThreads, 4) k_idct(DecodeLaunch d) {
         bool any = false;
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-            const uint32_t k = 8u * v + u;
-            row[u] = __fmul_rn(__int2float_rn(src[nb * scan[k] + blk]), sc[k]);
+            const uint32_t kk = 8u * v + u;
+            row[u] = __fmul_rn(__int2float_rn(src[nb * scan[kk] + blk]), sc[kk]);
             any |= row[u] != 0.0f;
         }
-        const uint32_t gblk = comp_start[c] / 64u + blk;
-        nz[gblk * 8u + v] = any;
+        held_any[k] = any;
         if (any) {
-            float *dst = tmp + comp_start[c];
 #pragma unroll
             for (int x = 0; x < 8; x++) {
-                float s = 0.0f;
+                float acc = 0.0f;
 #pragma unroll
-                for (int u = 0; u < 8; u++) s = __fadd_rn(s, __fmul_rn(row[u], c_idct_basis[8 * x + u]));
-                dst[(v * 8u + x) * nb + blk] = s;
+                for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, __fmul_rn(row[u], c_idct_basis[8 * x + u]));
+                held[k][x] = acc;
             }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; k++) {
+        const uint32_t t = tid + (uint32_t)k * kIdctThreads;
+        if (t >= all_blocks * 8u) continue;
+        const uint32_t c = t < comp_blocks[0] * 8u ? 0u : (t < (comp_blocks[0] + comp_blocks[1]) * 8u ? 1u : 2u);
+        const uint32_t tc = t - (c == 0 ? 0u : (c == 1 ? comp_blocks[0] * 8u : (comp_blocks[0] + comp_blocks[1]) * 8u));
+        const uint32_t nb = comp_blocks[c];
+        const uint32_t blk = tc % nb, v = tc / nb;
+        nz[(comp_start[c] / 64u + blk) * 8u + v] = held_any[k];
+        if (held_any[k]) {
+            float *dst = tmp + comp_start[c];
+#pragma unroll
+            for (int x = 0; x < 8; x++) dst[(v * 8u + x) * nb + blk] = held[k][x];
         }
     }
     __syncthreads();
@@ -721,7 +745,7 @@ cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cud
     return cudaGetLastError();
 }
 
-size_t idct_smem_bytes() { return 8 * kMaxSliceCoefs + 8 * (kMaxSliceCoefs / 64); }
+size_t idct_smem_bytes() { return 4 * kMaxSliceCoefs + 8 * (kMaxSliceCoefs / 64); }
 
 cudaError_t launch_idct(const DecodeLaunch &d, cudaStream_t s) {
     if (d.n_slices == 0) return cudaSuccess;
