@@ -1181,9 +1181,23 @@ struct BitOut {
     }
 };
 
+// The writer's tables: beside the code lengths, the codewords (their
+// significant bits) of run and level symbols below 32 by context.
+struct CodeTables : LenTables {
+    uint32_t run_code[16][32];
+    uint32_t level_code[9][32];
+    __device__ void fill_all() {
+        fill();
+        for (uint32_t i = threadIdx.x; i < 16 * 32; i += blockDim.x)
+            run_code[i >> 5][i & 31] = (uint32_t)cb_bits(run_book(i >> 5), i & 31);
+        for (uint32_t i = threadIdx.x; i < 9 * 32; i += blockDim.x)
+            level_code[i >> 5][i & 31] = (uint32_t)cb_bits(level_book(i >> 5), i & 31);
+    }
+};
+
 // One quantised component's codes (src/encode.rs:413-437), one lane.
 __device__ void lane_component_write(BitOut &w, const float *f, const float *cmax, uint32_t n_blocks,
-                                     const CompQuant &q, const LenTables &t) {
+                                     const CompQuant &q, const CodeTables &t) {
     const float inv0 = __ldg(q.inv);
     int32_t prev_dc = 0, prev_diff = 3;
     for (uint32_t i = 0; i < n_blocks; i++) {
@@ -1203,6 +1217,16 @@ __device__ void lane_component_write(BitOut &w, const float *f, const float *cma
         prev_dc = q;
     }
     ac_walk_sparse(f, cmax, n_blocks, q, [&](const AcWalk &a, uint32_t run, uint32_t level, bool neg) {
+        // Run, level and sign in one field, from the tables, when they can.
+        if (run < 32u && level < 32u) {
+            const uint32_t rc = min(a.prev_run, 15u), lc = min(a.prev_level, 8u);
+            const uint32_t rl = t.run[rc][run], ll = t.level[lc][level];
+            if (rl + ll + 1u <= 32u) {
+                w.put((((uint64_t)t.run_code[rc][run] << ll | t.level_code[lc][level]) << 1) | (uint64_t)neg,
+                      rl + ll + 1u);
+                return;
+            }
+        }
         const Codebook rb = run_book(a.prev_run), lb = level_book(a.prev_level);
         const uint32_t rl = t.run_len(a.prev_run, run), ll = t.level_len(a.prev_level, level);
         // Run, level and sign in one field when they fit.
@@ -1219,8 +1243,8 @@ __device__ void lane_component_write(BitOut &w, const float *f, const float *cma
 
 // Each slice component's codes, one lane per (component, slice).
 __global__ void __launch_bounds__(kCostThreads) k_pack(EncodeLaunch e) {
-    __shared__ LenTables t;
-    t.fill();
+    __shared__ CodeTables t;
+    t.fill_all();
     __syncthreads();
     const uint32_t item = blockIdx.x * kCostThreads + threadIdx.x;
     if (item >= 3u * e.n_slices) return;
