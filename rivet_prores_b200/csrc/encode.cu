@@ -517,6 +517,118 @@ __device__ uint32_t lane_component_bits(const float *f, const float *cmax, uint3
     return dc_bits(f, n_blocks, __ldg(q.inv)) + c.bits;
 }
 
+// Code lengths of a run and of a level by context, from the tables when
+// they hold the symbol (src/vlc.rs:397-415).
+__device__ __forceinline__ uint32_t run_len_of(const LenTables &t, uint32_t ctx, uint32_t r) {
+    return r < 32u ? t.run[ctx][r] : cb_len(run_book(ctx), r);
+}
+__device__ __forceinline__ uint32_t level_len_of(const LenTables &t, uint32_t ctx, uint32_t l) {
+    return l < 32u ? t.level[ctx][l] : cb_len(level_book(ctx), l);
+}
+
+// Bits of one quantised component (src/encode.rs:398-409), split over a
+// group of kSeg lanes, for short launches bound by one lane's walk: lane r
+// walks the r-th run of chunks as if the walk started there (previous run
+// 4, previous level 1, last position its start), which gets every code
+// right but the segment's first (run and level by the previous segment's
+// state) and its second's run (by the first's run). Lanes past the first
+// also find their segment's first two non-zeros, and the group's first
+// lane puts the segments together in order, replacing those codes with the
+// right ones: the sum is the one-lane walk's. Every lane of the warp takes
+// part (the exchange is by shuffles); `active` is false for lanes past the
+// work.
+template <int kSeg>
+__device__ uint32_t group_component_bits(bool active, const float *f, const float *cmax, uint32_t nb,
+                                         const CompQuant &q, const LenTables &t) {
+    const uint32_t lane = threadIdx.x & 31u, r = lane % (uint32_t)kSeg, base = lane - r;
+    const uint32_t chunks = active ? 2u * nb : 0u;
+    const uint32_t c_lo = chunks * r / kSeg, c_hi = chunks * (r + 1) / kSeg;
+    const uint32_t shift = active ? 31u - __clz(nb) : 0u;
+    const uint32_t start = r == 0 ? nb : 32u * c_lo;
+    AcCount c;
+    c.pos = start;
+    for (uint32_t k = c_lo; k < c_hi; k++) {
+        if (chunk_is_zero(cmax, q, k)) continue;
+        const uint32_t c0 = 32u * k;
+        if (nb >= 4) {
+            for (uint32_t p0 = max(c0, nb); p0 < c0 + 32u; p0 += 4) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+                const float iv = __ldg(q.inv + (p0 >> shift));
+                count_position(c, v.x, iv, p0, t);
+                count_position(c, v.y, iv, p0 + 1, t);
+                count_position(c, v.z, iv, p0 + 2, t);
+                count_position(c, v.w, iv, p0 + 3, t);
+            }
+        } else {
+            for (uint32_t p0 = c0; p0 < c0 + 32u; p0 += 4) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(f + p0));
+                const float ia = __ldg(q.inv + (p0 >> 1)), ib = __ldg(q.inv + (p0 >> 1) + 1);
+                if (p0 > 0) {
+                    count_position(c, v.x, ia, p0, t);
+                    count_position(c, v.y, ia, p0 + 1, t);
+                }
+                count_position(c, v.z, ib, p0 + 2, t);
+                count_position(c, v.w, ib, p0 + 3, t);
+            }
+        }
+    }
+    // The segment's first two non-zeros (lanes past the first).
+    uint32_t found = 0, q1 = 0, l1 = 0, q2 = 0;
+    if (r > 0) {
+        for (uint32_t k = c_lo; k < c_hi && found < 2u; k++) {
+            if (chunk_is_zero(cmax, q, k)) continue;
+            for (uint32_t p = 32u * k; p < 32u * k + 32u && found < 2u; p++) {
+                const float x = __fmul_rn(__ldg(f + p), __ldg(q.inv + (p >> shift)));
+                const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
+                if (m >= 1.0f) {
+                    if (found == 0) {
+                        q1 = p;
+                        l1 = (uint32_t)__float2int_rz(m) - 1u;
+                    } else {
+                        q2 = p;
+                    }
+                    found++;
+                }
+            }
+        }
+    }
+    // Put the segments together on the group's first lane.
+    uint32_t bits = c.bits, pos = c.pos, rctx = c.run_ctx, lctx = c.level_ctx;
+#pragma unroll
+    for (int j = 1; j < kSeg; j++) {
+        const uint32_t src = base + (uint32_t)j;
+        const uint32_t s_bits = __shfl_sync(0xffffffffu, c.bits, src);
+        const uint32_t s_found = __shfl_sync(0xffffffffu, found, src);
+        const uint32_t s_q1 = __shfl_sync(0xffffffffu, q1, src);
+        const uint32_t s_l1 = __shfl_sync(0xffffffffu, l1, src);
+        const uint32_t s_q2 = __shfl_sync(0xffffffffu, q2, src);
+        const uint32_t s_start = __shfl_sync(0xffffffffu, start, src);
+        const uint32_t s_pos = __shfl_sync(0xffffffffu, c.pos, src);
+        const uint32_t s_rctx = __shfl_sync(0xffffffffu, c.run_ctx, src);
+        const uint32_t s_lctx = __shfl_sync(0xffffffffu, c.level_ctx, src);
+        if (r == 0 && s_found > 0) {
+            const uint32_t run1 = s_q1 - pos, run1_seg = s_q1 - s_start;
+            // The first code: right contexts and run, in place of the
+            // segment's own (unsigned arithmetic: the sum comes out right).
+            bits += s_bits + run_len_of(t, rctx, run1) + level_len_of(t, lctx, s_l1) -
+                    run_len_of(t, 4u, run1_seg) - level_len_of(t, 1u, s_l1);
+            if (s_found == 1) {
+                pos = s_q1 + 1u;
+                rctx = min(run1, 15u);
+                lctx = min(s_l1, 8u);
+            } else {
+                // The second code's run by the first's right run.
+                const uint32_t run2 = s_q2 - s_q1 - 1u;
+                bits += run_len_of(t, min(run1, 15u), run2) - run_len_of(t, min(run1_seg, 15u), run2);
+                pos = s_pos;
+                rctx = s_rctx;
+                lctx = s_lctx;
+            }
+        }
+    }
+    return (r == 0 && active) ? dc_bits(f, nb, __ldg(q.inv)) + bits : 0u;
+}
+
 // The same count with a whole warp on one component, for when latency
 // matters more than throughput (few items, or one slice the share-out
 // needs): lane l takes scanned positions 32 k + l; a non-zero's run and its
@@ -713,28 +825,45 @@ __global__ void __launch_bounds__(kCostThreads) k_window_select(EncodeLaunch e, 
 
 // Costs the listed slices at window level `level` (quantiser uniform - 1 -
 // level): a lane per (component, slice), component-major, or a warp each.
+// Lanes per component in the window levels' lane mode: these launches cover
+// candidate lists, too short to fill the GPU, so a component's walk is
+// split to cut the launch's length.
+constexpr int kWindowSegments = 4;
+
 template <bool kWarp>
 __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, int level) {
     __shared__ LenTables t;
     const uint32_t n = e.win_count[level];
-    if (blockIdx.x * (kWarp ? kCostThreads / 32 : kCostThreads) >= 3u * n) return;  // the whole block
+    if (blockIdx.x * (kWarp ? kCostThreads / 32 : kCostThreads / kWindowSegments) >= 3u * n) return;  // the whole block
     t.fill();
     __syncthreads();
-    const uint32_t item = kWarp ? blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5)
-                                : blockIdx.x * kCostThreads + threadIdx.x;
-    if (item >= 3u * n) return;
-    const uint32_t comp = kWarp ? item % 3u : item / n;
-    const uint32_t s = e.win_list[kWarp ? item / 3u : item - comp * n];
-    const EncSliceDesc sd = e.slices[s];
-    const uint32_t qi = (uint32_t)(e.state[sd.pic].uniform - 1 - level);
-    const EncPicDesc &pd = e.pics[sd.pic];
-    const EncFrameDesc &fd = e.frames[pd.frame];
-    uint32_t *out = e.win_comp + ((uint64_t)level * e.n_slices + s) * 3u;
     if (kWarp) {
-        const uint32_t bytes = warp_component_bytes(e, sd, pd, fd, comp, qi, t);
-        if ((threadIdx.x & 31) == 0) out[comp] = bytes;
+        const uint32_t item = blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5);
+        if (item >= 3u * n) return;
+        const uint32_t comp = item % 3u, s = e.win_list[item / 3u];
+        const EncSliceDesc sd = e.slices[s];
+        const uint32_t qi = (uint32_t)(e.state[sd.pic].uniform - 1 - level);
+        const EncPicDesc &pd = e.pics[sd.pic];
+        const uint32_t bytes = warp_component_bytes(e, sd, pd, e.frames[pd.frame], comp, qi, t);
+        if ((threadIdx.x & 31) == 0) e.win_comp[((uint64_t)level * e.n_slices + s) * 3u + comp] = bytes;
     } else {
-        out[comp] = component_bytes(e, sd, pd, fd, comp, qi, t);
+        const uint32_t thread = blockIdx.x * kCostThreads + threadIdx.x;
+        if ((thread & ~31u) / kWindowSegments >= 3u * n) return;  // the whole warp
+        const uint32_t item = thread / kWindowSegments;
+        const bool active = item < 3u * n;
+        const uint32_t comp = active ? item / n : 0u;
+        const uint32_t s = e.win_list[active ? item - comp * n : 0u];
+        const EncSliceDesc sd = e.slices[s];
+        const uint32_t qi = active ? (uint32_t)(e.state[sd.pic].uniform - 1 - level) : 1u;
+        const EncPicDesc &pd = e.pics[sd.pic];
+        const EncFrameDesc &fd = e.frames[pd.frame];
+        uint32_t nb, off;
+        comp_layout(fd, sd.mbs, comp, nb, off);
+        const uint32_t bits = group_component_bits<kWindowSegments>(active, e.coef + sd.coef + off,
+                                                                    e.coef_max + ((sd.coef + off) >> 5), nb,
+                                                                    comp_quant(quant_base(e, pd, qi), comp, nb), t);
+        if (active && thread % kWindowSegments == 0)
+            e.win_comp[((uint64_t)level * e.n_slices + s) * 3u + comp] = (bits + 7u) / 8u;
     }
 }
 
@@ -1359,7 +1488,8 @@ cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s)
     if (err != cudaSuccess) return err;
     // The grid covers every slice; blocks past the list's end return.
     if (lane_mode(e))
-        k_cost_window<false><<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, level);
+        k_cost_window<false><<<(items * kWindowSegments + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(
+            e, level);
     else
         k_cost_window<true><<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, level);
     return cudaGetLastError();
