@@ -70,11 +70,14 @@ __device__ __forceinline__ void put_field(uint32_t *out, uint64_t bitpos, uint64
     }
 }
 
+// floor(|x| + r) as an integer: |x| + r is positive, so truncation is the
+// floor (and both saturate alike from 2^31 up).
+__device__ __forceinline__ int32_t magnitude(float x, float r) { return __float2int_rz(__fadd_rn(fabsf(x), r)); }
+
 __device__ __forceinline__ int32_t quantise1(float f, float inv, float r) {
     // x = F inv; QF = sign(x) floor(|x| + r) (src/dsp/scalar.rs:19-39).
     const float x = __fmul_rn(f, inv);
-    const float m = floorf(__fadd_rn(fabsf(x), r));
-    const int32_t q = __float2int_rz(m);
+    const int32_t q = magnitude(x, r);
     return x < 0.0f ? -q : q;
 }
 
@@ -366,9 +369,8 @@ __device__ __forceinline__ uint32_t dc_bits(const float *f, uint32_t n_blocks, f
 }
 
 // One AC position of a lane's walk: x = F inv, m = floor(|x| + 0.42)
-// (src/dsp/scalar.rs:19-39), tested for zero in float; only a non-zero
-// coefficient is converted and coded (its run from the last one, its level,
-// both by context).
+// (src/dsp/scalar.rs:19-39) as an integer; only a non-zero coefficient is
+// coded (its run from the last one, its level, both by context).
 struct AcWalk {
     uint32_t prev_run = 4, prev_level = 1, pos = 0;
 };
@@ -376,10 +378,10 @@ struct AcWalk {
 template <class Emit>
 __device__ __forceinline__ void ac_position(AcWalk &w, float f, float inv, uint32_t p, Emit emit) {
     const float x = __fmul_rn(f, inv);
-    const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
-    if (m >= 1.0f) {
+    const int32_t m = magnitude(x, kAcRounding);
+    if (m >= 1) {
         const uint32_t run = p - w.pos;
-        const uint32_t level = (uint32_t)__float2int_rz(m) - 1u;
+        const uint32_t level = (uint32_t)m - 1u;
         emit(w, run, level, x < 0.0f);
         w.prev_run = run;
         w.prev_level = level;
@@ -491,11 +493,10 @@ struct AcCount {
 };
 
 __device__ __forceinline__ void count_position(AcCount &c, float f, float inv, uint32_t p, const LenTables &t) {
-    const float x = __fmul_rn(f, inv);
-    const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
-    const bool nz = m >= 1.0f;
+    const int32_t m = magnitude(__fmul_rn(f, inv), kAcRounding);
+    const bool nz = m >= 1;
     const uint32_t run = p - c.pos;
-    const uint32_t level = (uint32_t)__float2int_rz(m) - 1u;
+    const uint32_t level = (uint32_t)m - 1u;
     uint32_t add = (uint32_t)t.run[c.run_ctx][min(run, 31u)] + (uint32_t)t.level[c.level_ctx][min(level, 31u)] + 1u;
     if (nz && (run | level) >= 32u)
         add = cb_len(run_book(c.run_ctx), run) + cb_len(level_book(c.level_ctx), level) + 1u;
@@ -578,12 +579,11 @@ __device__ uint32_t group_component_bits(bool active, const float *f, const floa
         for (uint32_t k = c_lo; k < c_hi && found < 2u; k++) {
             if (chunk_is_zero(cmax, q, k)) continue;
             for (uint32_t p = 32u * k; p < 32u * k + 32u && found < 2u; p++) {
-                const float x = __fmul_rn(__ldg(f + p), __ldg(q.inv + (p >> shift)));
-                const float m = floorf(__fadd_rn(fabsf(x), kAcRounding));
-                if (m >= 1.0f) {
+                const int32_t m = magnitude(__fmul_rn(__ldg(f + p), __ldg(q.inv + (p >> shift))), kAcRounding);
+                if (m >= 1) {
                     if (found == 0) {
                         q1 = p;
-                        l1 = (uint32_t)__float2int_rz(m) - 1u;
+                        l1 = (uint32_t)m - 1u;
                     } else {
                         q2 = p;
                     }
