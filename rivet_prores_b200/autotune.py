@@ -217,10 +217,9 @@ def tune(device: int = 0, quick: bool = False, store: bool = True, frames: Optio
 
     # Staging depth of the host round trip.
     ctx.set_tuning(tuning)
-    depths = {}
     stage_frames = stage_frames or frames
     timed = {}
-    for d in depths or ([2, 4, 8] if quick else [2, 4, 8, 16]):
+    for d in depths or ([2, 3, 4, 6, 8] if quick else [2, 3, 4, 6, 8, 16]):
         if d > len(stage_frames):
             continue
         pipe = RoundTripPipeline(stage_frames, cfg, d, device=device)

@@ -373,7 +373,7 @@ Status upload_encode(Context &ctx, Workspace &ws, EncodePlan &plan, const prores
         PR_CUDA(ws.slices.reserve(sizeof(EncSliceDesc) * (plan.n_slices + 1)), "cudaMalloc");
         PR_CUDA(ws.enc_pic_state.reserve(sizeof(EncPicState) * (plan.pdesc.size() + 1)), "cudaMalloc");
         // The coefficients, then (64 floats on) one chunk maximum per 32.
-    PR_CUDA(ws.enc_coef.reserve(4 * (plan.coef_total + plan.coef_total / 32 + 128)), "cudaMalloc coefficients");
+        PR_CUDA(ws.enc_coef.reserve(4 * (plan.coef_total + plan.coef_total / 32 + 128)), "cudaMalloc coefficients");
         PR_CUDA(ws.weights.reserve(4 * (plan.quant.size() + 64)), "cudaMalloc");
         PR_CUDA(ws.enc_cost.reserve(cost_bytes(plan)), "cudaMalloc");
         PR_CUDA(ws.enc_out.reserve(plan.out_total + 64), "cudaMalloc output");

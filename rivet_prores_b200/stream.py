@@ -12,6 +12,7 @@ stay in pinned host memory, so every copy is a DMA at full PCIe rate.
 from __future__ import annotations
 
 import concurrent.futures as cf
+import threading
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -23,9 +24,14 @@ class RoundTripPipeline:
 
     `run(steps)` streams the batch through `steps` times: every part copies
     its frames in from pinned memory, runs both directions and copies its
-    planes out, then starts over, each part at its own pace, so that one
-    step's downloads overlap the next step's uploads. The last packets
-    (views into pinned staging, valid until the next run) and decoded planes
+    planes out, then starts over, each part at its own pace. A part's next
+    frames go up on its own upload stream as soon as its encode has read the
+    last ones, so they overlap its decode and download; uploads of all
+    parts queue in one order (each waits for the one issued before it), so
+    the copy engine finishes one part's frames at a time and the parts fall
+    into step behind one another instead of all uploading, then all
+    encoding, then all downloading at once. The last packets (views into
+    pinned staging, valid until the next run) and decoded planes
     (`self.planes`, one pinned row per frame) stay. It returns (start, end)
     CUDA events on `self.stream` that bracket the run on the device."""
 
@@ -62,17 +68,40 @@ class RoundTripPipeline:
                     raise p
             dec = DecodeJob([bytes(p) for p in packets], device=device)
             self.parts.append({"enc": enc, "dec": dec, "frames": hframes, "stream": torch.cuda.Stream(device),
+                               "up": torch.cuda.Stream(device),
                                "arrays": [(self.planes[i], None) for i in range(lo, hi)]})
         self.stream = torch.cuda.Stream(device)
         self.pool = cf.ThreadPoolExecutor(max_workers=depth)
         self.packets: List[memoryview] = []
+        self._order = threading.Lock()
+        self._last_upload = None
+
+    def _upload(self, part):
+        """Queues the part's frames behind the last upload of any part."""
+        up = part["up"]
+        with self._order:
+            if self._last_upload is not None:
+                up.wait_event(self._last_upload)
+            part["enc"].upload(part["frames"], up)
+            done = self.torch.cuda.Event()
+            done.record(up)
+            self._last_upload = done
+        part["uploaded"] = done
 
     def _part(self, part, steps: int):
-        st = part["stream"]
+        st, up = part["stream"], part["up"]
         pk = []
-        for _ in range(steps):
-            part["enc"].upload(part["frames"], st)
+        self._upload(part)
+        for k in range(steps):
+            st.wait_event(part["uploaded"])
             part["enc"].launch(st, graph=True)
+            if k + 1 < steps:
+                # The next frames may overwrite the input once this encode
+                # has run.
+                read = self.torch.cuda.Event()
+                read.record(st)
+                up.wait_event(read)
+                self._upload(part)
             pk = part["enc"].fetch(st, copy=False)
             part["dec"].upload([np.frombuffer(p, dtype=np.uint8) for p in pk], st)
             part["dec"].launch(st, graph=True)
@@ -84,8 +113,10 @@ class RoundTripPipeline:
         torch = self.torch
         start = torch.cuda.Event(enable_timing=True)
         start.record(self.stream)
+        self._last_upload = None
         for part in self.parts:
             part["stream"].wait_event(start)
+            part["up"].wait_event(start)
             part["end"] = torch.cuda.Event(enable_timing=True)
         outs = list(self.pool.map(lambda p: self._part(p, steps), self.parts))
         for part in self.parts:
