@@ -573,13 +573,12 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
 
     // Row pass: tmp[v][x] = sum_u F[v][u] T[x][u], u in order, from 0
     // (src/dct.rs:38-53); all-zero rows are skipped, as the crate does.
-    uint32_t comp_start[3], comp_blocks[3];
-    comp_blocks[0] = 4u * mbs;
-    comp_blocks[1] = comp_blocks[2] = cpm * mbs;
-    comp_start[0] = 0;
-    comp_start[1] = 64u * comp_blocks[0];
-    comp_start[2] = comp_start[1] + 64u * comp_blocks[1];
-    const uint32_t all_blocks = comp_blocks[0] + 2u * comp_blocks[1];
+    // Blocks of a component and its first coefficient in the slice (by
+    // select, not an indexed array, which would live in local memory).
+    const uint32_t luma_blocks = 4u * mbs, chroma_blocks = cpm * mbs;
+    const auto blocks_of = [&](uint32_t c) { return c == 0 ? luma_blocks : chroma_blocks; };
+    const auto start_of = [&](uint32_t c) { return c == 0 ? 0u : 64u * (luma_blocks + (c - 1u) * chroma_blocks); };
+    const uint32_t all_blocks = luma_blocks + 2u * chroma_blocks;
     // The row results are held in registers until every thread has read
     // its coefficients, then written over them (the two arrays share the
     // shared memory, so that five CTAs fit on an SM).
@@ -591,11 +590,11 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t t = tid + (uint32_t)k * kIdctThreads;
         held_any[k] = false;
         if (t >= all_blocks * 8u) continue;
-        const uint32_t c = t < comp_blocks[0] * 8u ? 0u : (t < (comp_blocks[0] + comp_blocks[1]) * 8u ? 1u : 2u);
-        const uint32_t tc = t - (c == 0 ? 0u : (c == 1 ? comp_blocks[0] * 8u : (comp_blocks[0] + comp_blocks[1]) * 8u));
-        const uint32_t nb = comp_blocks[c];
+        const uint32_t c = t < luma_blocks * 8u ? 0u : (t < (luma_blocks + chroma_blocks) * 8u ? 1u : 2u);
+        const uint32_t tc = t - start_of(c) / 8u;  // 8 row tasks a block
+        const uint32_t nb = blocks_of(c);
         const uint32_t blk = tc % nb, v = tc / nb;
-        const int32_t *src = cs + comp_start[c];
+        const int32_t *src = cs + start_of(c);
         const float *sc = scale[c > 0];
         float row[8];
         bool any = false;
@@ -621,28 +620,65 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
     for (int k = 0; k < kRowsPerThread; k++) {
         const uint32_t t = tid + (uint32_t)k * kIdctThreads;
         if (t >= all_blocks * 8u) continue;
-        const uint32_t c = t < comp_blocks[0] * 8u ? 0u : (t < (comp_blocks[0] + comp_blocks[1]) * 8u ? 1u : 2u);
-        const uint32_t tc = t - (c == 0 ? 0u : (c == 1 ? comp_blocks[0] * 8u : (comp_blocks[0] + comp_blocks[1]) * 8u));
-        const uint32_t nb = comp_blocks[c];
+        const uint32_t c = t < luma_blocks * 8u ? 0u : (t < (luma_blocks + chroma_blocks) * 8u ? 1u : 2u);
+        const uint32_t tc = t - start_of(c) / 8u;  // 8 row tasks a block
+        const uint32_t nb = blocks_of(c);
         const uint32_t blk = tc % nb, v = tc / nb;
-        nz[(comp_start[c] / 64u + blk) * 8u + v] = held_any[k];
+        nz[(start_of(c) / 64u + blk) * 8u + v] = held_any[k];
         if (held_any[k]) {
-            float *dst = tmp + comp_start[c];
+            float *dst = tmp + start_of(c);
 #pragma unroll
             for (int x = 0; x < 8; x++) dst[(v * 8u + x) * nb + blk] = held[k][x];
         }
     }
     __syncthreads();
 
-    // Column pass, conversion and store: out[y][x] = sum_v T[y][v] tmp[v][x]
-    // in order (src/dct.rs:54-64), then floor(v scale + bias) clamped
-    // (src/dsp/scalar.rs:8-12). A thread makes one 8-sample row of a block;
-    // neighbouring threads make neighbouring rows segments of the picture.
+    // Column pass and conversion: out[y][x] = sum_v T[y][v] tmp[v][x] in
+    // order (src/dct.rs:54-64), then floor(v scale + bias) clamped
+    // (src/dsp/scalar.rs:8-12). A task is two neighbouring columns of one
+    // block, so each row result is read once; neighbouring threads take
+    // neighbouring blocks (no bank conflicts). The samples go to shared
+    // memory as pairs, [y][column pair][blk] per component.
     const float oscale = fd.out_scale, obias = fd.out_bias, omax = fd.out_max;
+    uint32_t *stage = reinterpret_cast<uint32_t *>(smem + 4 * kMaxSliceCoefs + kMaxSliceCoefs / 8);
+    const auto convert = [&](float a) {
+        float v = floorf(__fadd_rn(__fmul_rn(a, oscale), obias));
+        v = v < 0.0f ? 0.0f : (v > omax ? omax : v);
+        return (uint32_t)v;
+    };
+    for (uint32_t t = tid; t < all_blocks * 4u; t += kIdctThreads) {
+        const uint32_t c = t < luma_blocks * 4u ? 0u : (t < (luma_blocks + chroma_blocks) * 4u ? 1u : 2u);
+        const uint32_t tc = t - start_of(c) / 16u;  // 4 column tasks a block
+        const uint32_t nb = blocks_of(c);
+        const uint32_t blk = tc % nb, j = tc / nb;
+        const float *src = tmp + start_of(c) + 2u * j * nb + blk;
+        const uint64_t rows = *reinterpret_cast<const uint64_t *>(nz + (start_of(c) / 64u + blk) * 8u);
+        float a0[8], a1[8];
+#pragma unroll
+        for (int y = 0; y < 8; y++) a0[y] = a1[y] = 0.0f;
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            if (!((rows >> (8 * v)) & 0xffu)) continue;
+            const float t0 = src[8u * v * nb], t1 = src[8u * v * nb + nb];
+#pragma unroll
+            for (int y = 0; y < 8; y++) {
+                const float w = c_idct_basis[8 * y + v];
+                a0[y] = __fadd_rn(a0[y], __fmul_rn(w, t0));
+                a1[y] = __fadd_rn(a1[y], __fmul_rn(w, t1));
+            }
+        }
+        uint32_t *dst = stage + start_of(c) / 2u + j * nb + blk;
+#pragma unroll
+        for (int y = 0; y < 8; y++) dst[4u * y * nb] = convert(a0[y]) | (convert(a1[y]) << 16);
+    }
+    __syncthreads();
+
+    // Stores: a thread writes one 8-sample row of a block; neighbouring
+    // threads write neighbouring row segments of the picture.
     for (uint32_t c = 0; c < 3; c++) {
         const uint32_t segs = (c == 0 || cpm == 4) ? 2u * mbs : mbs;
         const uint32_t per_mb = c == 0 ? 4u : cpm;
-        const uint32_t nb = comp_blocks[c];
+        const uint32_t nb = blocks_of(c);
         const uint32_t pw = fd.plane_w[c];
         uint16_t *plane = fd.out_planes ? fd.out_planes + (fd.plane_off[c] - fd.plane_off[0]) : d.planes + fd.plane_off[c];
         for (uint32_t t = tid; t < 16u * segs; t += kIdctThreads) {
@@ -662,36 +698,21 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
             uint32_t bx, by;
             block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, bb, bx, by);
             if (bx >= pw || by + y >= pd.height) continue;
-            const uint32_t gblk = comp_start[c] / 64u + blk;
-            const float *src = tmp + comp_start[c];
-            float acc[8];
-#pragma unroll
-            for (int x = 0; x < 8; x++) acc[x] = 0.0f;
-#pragma unroll
-            for (int v = 0; v < 8; v++) {
-                if (!nz[gblk * 8u + v]) continue;
-                const float w = c_idct_basis[8u * y + v];
-#pragma unroll
-                for (int x = 0; x < 8; x++) acc[x] = __fadd_rn(acc[x], __fmul_rn(w, src[(v * 8u + x) * nb + blk]));
-            }
-            uint16_t px[8];
-#pragma unroll
-            for (int x = 0; x < 8; x++) {
-                float s = floorf(__fadd_rn(__fmul_rn(acc[x], oscale), obias));
-                s = s < 0.0f ? 0.0f : (s > omax ? omax : s);
-                px[x] = (uint16_t)s;
-            }
+            const uint32_t *src = stage + start_of(c) / 2u + 4u * y * nb + blk;
+            uint4 v;
+            v.x = src[0];
+            v.y = src[nb];
+            v.z = src[2u * nb];
+            v.w = src[3u * nb];
             const uint32_t cols = min(8u, pw - bx);
             uint16_t *dst = plane + (uint64_t)(pd.first_row + pd.row_step * (by + y)) * pw + bx;
             if (cols == 8u && ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0)) {
-                uint4 v;
-                v.x = px[0] | ((uint32_t)px[1] << 16);
-                v.y = px[2] | ((uint32_t)px[3] << 16);
-                v.z = px[4] | ((uint32_t)px[5] << 16);
-                v.w = px[6] | ((uint32_t)px[7] << 16);
                 *reinterpret_cast<uint4 *>(dst) = v;
             } else {
-                for (uint32_t x = 0; x < cols; x++) dst[x] = px[x];
+                for (uint32_t x = 0; x < cols; x++) {
+                    const uint32_t w = x < 2u ? v.x : (x < 4u ? v.y : (x < 6u ? v.z : v.w));
+                    dst[x] = (uint16_t)(w >> (16u * (x & 1u)));
+                }
             }
         }
     }
@@ -745,7 +766,8 @@ cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cud
     return cudaGetLastError();
 }
 
-size_t idct_smem_bytes() { return 4 * kMaxSliceCoefs + 8 * (kMaxSliceCoefs / 64); }
+// Coefficients (row results over them), non-zero row flags, sample pairs.
+size_t idct_smem_bytes() { return 4 * kMaxSliceCoefs + kMaxSliceCoefs / 8 + 2 * kMaxSliceCoefs; }
 
 cudaError_t launch_idct(const DecodeLaunch &d, cudaStream_t s) {
     if (d.n_slices == 0) return cudaSuccess;
