@@ -42,11 +42,11 @@ ALGO_BYTES_PER_FRAME = 3_643_238 + 2 * (W * H * 2)
 # traffic grows with the frames a launch covers). k_cost is the mean of its
 # nine probe launches.
 PROFILED = {
-    "k_cost": {"dram_bytes_per_frame": 51.37e6, "issue_active_pct": "52-71"},
-    "k_idct": {"dram_bytes_per_frame": 73.01e6, "issue_active_pct": "66"},
-    "k_fdct": {"dram_bytes_per_frame": 97.76e6, "issue_active_pct": "83"},
-    "k_entropy": {"dram_bytes_per_frame": 71.34e6, "issue_active_pct": "44"},
-    "k_pack": {"dram_bytes_per_frame": 78.86e6, "issue_active_pct": "72"},
+    "k_cost": {"dram_bytes_per_frame": 51.29e6, "issue_active_pct": "39-54"},
+    "k_idct": {"dram_bytes_per_frame": 51.28e6, "issue_active_pct": "80"},
+    "k_fdct": {"dram_bytes_per_frame": 97.77e6, "issue_active_pct": "83"},
+    "k_entropy": {"dram_bytes_per_frame": 40.13e6, "issue_active_pct": "57"},
+    "k_pack": {"dram_bytes_per_frame": 78.75e6, "issue_active_pct": "61"},
 }
 
 
