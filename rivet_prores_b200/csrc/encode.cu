@@ -648,6 +648,17 @@ __device__ uint32_t group_component_bits(bool active, const float *f, const floa
 // needs): lane l takes scanned positions 32 k + l; a non-zero's run and its
 // contexts (the previous non-zero's run and level symbol) come from the
 // lanes below it or from what the last step carried.
+// kShared: f and cmax point into shared memory (plain loads); else into
+// global memory (read-only loads).
+template <bool kShared>
+__device__ __forceinline__ float coef_load(const float *f, uint32_t i) {
+    if constexpr (kShared)
+        return f[i];
+    else
+        return __ldg(f + i);
+}
+
+template <bool kShared = false>
 __device__ uint32_t warp_component_bits(const float *f, const float *cmax, uint32_t n_blocks, const CompQuant &cq,
                                         const LenTables &t) {
     const float *inv = cq.inv;
@@ -659,10 +670,10 @@ __device__ uint32_t warp_component_bits(const float *f, const float *cmax, uint3
     uint32_t carry_run = 4, carry_level = 1;
     for (uint32_t base = 0; base < total; base += 32) {
         // Past the DCs a chunk that quantises to zero changes nothing.
-        if (base > 0 && chunk_is_zero(cmax, cq, base >> 5)) continue;
+        if (base > 0 && coef_load<kShared>(cmax, base >> 5) < __ldg(cq.chunk + (base >> 5))) continue;
         const uint32_t p = base + lane;
         const uint32_t sidx = p >> shift;
-        const int32_t q = quantise1(__ldg(f + p), __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
+        const int32_t q = quantise1(coef_load<kShared>(f, p), __ldg(inv + sidx), sidx == 0 ? 0.5f : kAcRounding);
         if (base == 0) {
             // The DCs (n_blocks <= 32, all in this step).
             const int32_t left = __shfl_up_sync(0xffffffffu, q, 1);
@@ -1050,10 +1061,14 @@ __device__ __forceinline__ uint32_t steps_at(const SharePrep &p, uint64_t D, int
     return k;
 }
 
-constexpr int kShareWarps = 4;
+constexpr int kShareWarps = 1;
 
 __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     __shared__ LenTables t;
+    // The slice a deep step costs, copied in once (its coefficients, then
+    // its chunk maxima): the warp walks it for every quantiser it tries,
+    // and from DRAM each of its chunks waited out a full load.
+    __shared__ __align__(16) float stage[kShareWarps][kMaxSliceCoefs + kMaxSliceCoefs / 32];
     t.fill();
     __syncthreads();
     const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
@@ -1145,9 +1160,27 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
                 uint32_t c3[3] = {0, 0, 0};
                 int32_t qi = st.uniform - (int32_t)fk;
                 bool any = false;
+                float *sf = stage[threadIdx.x >> 5], *smax = sf + kMaxSliceCoefs;
+                const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+                const uint32_t total = 64u * (4u + 2u * cpm) * fsd.mbs;
+                if (qi > 1) {
+                    __syncwarp();  // the last deep slice's walks are over
+                    const float4 *src = reinterpret_cast<const float4 *>(e.coef + fsd.coef);
+#pragma unroll 4
+                    for (uint32_t i = (uint32_t)lane; i < total / 4u; i += 32u)
+                        reinterpret_cast<float4 *>(sf)[i] = __ldg(src + i);
+                    const float *msrc = e.coef_max + (fsd.coef >> 5);
+                    for (uint32_t i = (uint32_t)lane; i < total / 32u; i += 32u) smax[i] = __ldg(msrc + i);
+                    __syncwarp();
+                }
                 while (qi > 1) {
                     uint32_t n3[3];
-                    for (uint32_t c = 0; c < 3; c++) n3[c] = warp_component_bytes(e, fsd, pd, fd, c, (uint32_t)(qi - 1), t);
+                    for (uint32_t c = 0; c < 3; c++) {
+                        uint32_t nb, off;
+                        comp_layout(fd, fsd.mbs, c, nb, off);
+                        const CompQuant q = comp_quant(quant_base(e, pd, (uint32_t)(qi - 1)), c, nb);
+                        n3[c] = (warp_component_bits<true>(sf + off, smax + (off >> 5), nb, q, t) + 7u) / 8u;
+                    }
                     bool fits;
                     const uint64_t n = slice_total(hb, n3, alpha, fits);
                     if (!(fits && n <= allowed)) break;
