@@ -406,8 +406,10 @@ def run_b200(args):
 
 def run_serving(args, device):
     """Poisson requests (70 % decode, 30 % encode) over the heterogeneous
-    mix, served with continuous batching under an 8 GiB device budget; then
-    the same offered load served one request per launch."""
+    mix, served with continuous batching under an 8 GiB device budget, at
+    the offered rate (near what the server can take: throughput) and at half
+    of it (latency with headroom); then the full offered load served one
+    request per launch."""
     import numpy as np
 
     import rivet_prores_b200 as P
@@ -437,8 +439,10 @@ def run_serving(args, device):
                            "pooled page-locked buffers"}
     # Batches of at most 16: large enough to fill the device, small enough
     # that a request does not wait behind a long batch.
-    for name, workers, max_batch, seconds in [("batched", 4, 16, args.serve_seconds),
-                                              ("plain", 1, 1, max(1.0, args.serve_seconds / 4))]:
+    for name, workers, max_batch, seconds, rate in [
+            ("batched", 4, 16, args.serve_seconds, args.serve_rate),
+            ("batched_half_load", 4, 16, max(1.0, args.serve_seconds / 2), args.serve_rate / 2),
+            ("plain", 1, 1, max(1.0, args.serve_seconds / 4), args.serve_rate)]:
         # One backend (and its pool of page-locked output buffers) for the
         # warm-up and the measured run.
         backend = S.GpuBackend(device)
@@ -446,7 +450,7 @@ def run_serving(args, device):
         S.poisson_run(srv, maker(1), rate=200.0, seconds=0.3)  # workspaces allocated, not measured
         srv.close()
         srv = S.Server(backend, memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
-        st = S.poisson_run(srv, maker(2), rate=args.serve_rate, seconds=seconds)
+        st = S.poisson_run(srv, maker(2), rate=rate, seconds=seconds)
         srv.close()
         out[name] = st
     return out
