@@ -212,7 +212,7 @@ def run_b200(args):
     if not args.no_tune:
         from rivet_prores_b200 import autotune
 
-        autotune.tune(device=local, quick=True, store=False, frames=frames[:8], stage_frames=frames,
+        autotune.tune(device=local, quick=True, store=False, frames=frames, stage_frames=frames,
                       depths=[2, 3, 4, 6, 8])
         tuning_note = "tuned in this run (rivet_prores_b200.autotune, quick search)"
     from dataclasses import asdict
