@@ -7,7 +7,6 @@ number of parts."""
 import numpy as np
 import pytest
 
-import rivet_prores_b200 as P
 from oracle import oracle as O
 from rivet_prores_b200.stream import RoundTripPipeline
 from tests.util import to_config, to_frame
@@ -39,9 +38,3 @@ def test_round_trip_pipeline_matches_the_oracle(depth):
         assert up == down == 2 * pipe.host.size + sum(len(p) for p in pipe.packets)
     finally:
         pipe.close()
-
-
-def test_round_trip_pipeline_refuses_mixed_sizes():
-    frames = [to_frame(O.test_frame(64, 48, 2, 10, 12, 1)), to_frame(O.test_frame(80, 48, 2, 10, 12, 2))]
-    with pytest.raises(ValueError):
-        RoundTripPipeline(frames, P.Config(P.Profile.Hq), 2)
