@@ -3,19 +3,23 @@
 One step = encode a batch of B 3840x2160 4:2:2 10-bit frames as 422 HQ
 (apch, target 3 643 238 B each) and decode the B packets back to planes,
 each direction one batched, CUDA-graph-captured launch on device-resident
-buffers. `value` is frames/s through both directions (B per step);
-decode-only and encode-only rates, the plain one-frame-per-launch forms,
-and the end-to-end rate through the C ABI with host buffers (`e2e`) are
+buffers. `value` is frames/s through both directions (B distinct pictures
+per step); decode-only and encode-only rates, the plain one-frame-per-launch
+forms, the end-to-end rate through the C ABI with host buffers (`e2e`), the
+other benchmark configurations (`configs`), serving under a Poisson request
+stream (`serve`) and the CPU codec on the host's cores (`cpu_baseline`) are
 reported beside it. Inputs are seeded synthetic pictures
 (rivet_prores_b200/workloads.py); every step's inputs (B x 33 MB of planes)
 are larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl b200|reference]
 
-Under torchrun each rank codes its own batch (weak scaling, no collective
-on the data path); times are the max over ranks. `--impl reference` times
-the reference codec's CPU path (the oracle's restatement of it, with its
-slice-parallel thread pool on every host core) on the same workload.
+Under torchrun each rank codes its share of a global batch of B x N frames,
+split by macroblock count as the library's multi-device calls split it
+(weak scaling, no collective on the data path); times are the max over
+ranks. `--impl reference` times the reference codec's CPU path (the
+oracle's restatement of it, with its slice-parallel thread pool on every
+host core) on the same workload.
 """
 
 from __future__ import annotations
@@ -34,19 +38,28 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ProRes UHD HQ frames/s on 1 B200, bit-exact; batched vs plain; serve p50/p99"
 W, H = 3840, 2160
-# Algorithmic bytes per frame and direction: the packet (3 643 238 B at the
-# 422 HQ target) plus the 16.59 M u16 samples of the planes.
-ALGO_BYTES_PER_FRAME = 3_643_238 + 2 * (W * H * 2)
-# DRAM bytes (read + write) per frame and launch, and issue-slot use, from
-# one ncu capture of 14 UHD 422 HQ frames (profiles/kernels_uhd_422hq_b14.md;
-# traffic grows with the frames a launch covers). k_cost is the mean of its
-# nine probe launches.
-PROFILED = {
-    "k_cost": {"dram_bytes_per_frame": 51.29e6, "issue_active_pct": "39-54"},
-    "k_idct": {"dram_bytes_per_frame": 51.28e6, "issue_active_pct": "80"},
-    "k_fdct": {"dram_bytes_per_frame": 97.77e6, "issue_active_pct": "83"},
-    "k_entropy": {"dram_bytes_per_frame": 40.13e6, "issue_active_pct": "57"},
-    "k_pack": {"dram_bytes_per_frame": 78.75e6, "issue_active_pct": "61"},
+SAMPLES = W * H * 2  # u16 samples of a 4:2:2 frame: Y' plus two half-width chroma planes
+TARGET = 3_643_238  # Profile::target_frame_bytes(HQ, 3840, 2160)
+
+# Each kernel's own algorithmic bytes per frame and launch, for a frame of
+# `s` u16 samples coded into a packet of `p` bytes (the encoder's
+# coefficients are f32 in the slice's scanned order, plus one f32 maximum
+# per 32 of them; the decoder reads the packet once and writes the planes).
+KERNEL_BYTES = {
+    "k_fdct": (lambda s, p: 2 * s + 4 * s + s // 8, "planes in (2 B a sample), f32 coefficients and chunk maxima out"),
+    "k_cost": (lambda s, p: 4 * s + s // 8, "f32 coefficients and chunk maxima a probe reads when it skips no chunk"),
+    "k_cost_window": (lambda s, p: 4 * s + s // 8, "f32 coefficients and chunk maxima, every slice costed"),
+    "k_pack": (lambda s, p: 4 * s + s // 8 + p, "f32 coefficients and chunk maxima in, packet out"),
+    "k_decode": (lambda s, p: p + 2 * s, "packet in, u16 planes out"),
+    "k_entropy": (lambda s, p: p, "packet in (coefficient lists are an intermediate)"),
+    "k_idct": (lambda s, p: 2 * s, "u16 planes out (coefficient lists are an intermediate)"),
+}
+# Figures from ncu captures of these kernels, not measured by this run: the
+# capture's DRAM bytes (read + write) per frame and launch, and issue-slot use.
+CAPTURED = {
+    "k_cost": {"dram_bytes_per_frame": 51.29e6, "issue_active_pct": "39-54",
+               "capture": "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,... on a 14-frame UHD 422 HQ "
+                          "encode, mean of its 9 probe launches"},
 }
 
 
@@ -56,14 +69,16 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--unique", type=int, default=4, help="distinct synthetic pictures in a batch")
+    ap.add_argument("--unique", type=int, default=0, help="distinct pictures in a batch (0: all of them)")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-chunks", type=int, default=0,
                     help="parts the end-to-end batch is split over (0: the tuned staging depth)")
     ap.add_argument("--no-tune", action="store_true", help="keep the cached or default launch shapes")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=8.0, help="0 skips the serving run")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other benchmark configurations")
+    ap.add_argument("--no-check", action="store_true", help="skip the bit-exactness checks against the oracle")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="0 skips the serving run")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="mean requests/s (Poisson)")
     return ap.parse_args()
 
@@ -119,24 +134,81 @@ class Clocks:
                 "power_w_max": max(float(r[4]) for r in mine if r[4].replace(".", "").isdigit())}
 
 
-def cpu_baseline(frames, cfg_oracle, reps=3):
-    """The oracle's slice-parallel CPU codec on every host core: best of
-    `reps` runs over the sample, encode then decode of each frame."""
+# ---------------------------------------------------------------- CPU codec
+
+def _oracle_pic(f):
     from oracle import oracle as O
 
-    pics = [O.Picture(f.width, f.height, f.bit_depth, f.chroma.value, f.interlace.value, (0, 0, 2, 2, 2),
-                      f.data, None) for f in frames]
+    return O.Picture(f.width, f.height, f.bit_depth, f.chroma.value, f.interlace.value,
+                     (f.metadata.aspect_ratio, f.metadata.frame_rate_code, f.metadata.color_primaries,
+                      f.metadata.transfer_characteristic, f.metadata.matrix_coefficients), f.data, f.alpha)
+
+
+def _oracle_cfg(c):
+    from oracle import oracle as O
+
+    return O.Config(c.profile.value, c.log2_slice_mbs, c.alpha.value, c.luma_matrix, c.chroma_matrix,
+                    c.target_frame_bytes, c.encoder_identifier)
+
+
+def _best(fn, reps):
     best = None
     for _ in range(reps):
         t = time.perf_counter()
-        for p in pics:
-            k, msg, pkt = O.encode(cfg_oracle, p)
-            assert k == 0, msg
-            k, msg, d = O.decode(pkt)
-            assert k == 0, msg
+        fn()
         dt = time.perf_counter() - t
         best = dt if best is None else min(best, dt)
-    return len(pics) / best, os.cpu_count()
+    return best
+
+
+def cpu_codec_rates(frames, cfg, threads: int, reps: int = 5):
+    """The oracle's CPU codec (the crate's slice-parallel path, restated) on
+    `threads` host threads (0: all): encode and decode timed separately,
+    best of `reps`, with the pictures and packets prepared outside the
+    timed region. Returns (encode fps, decode fps)."""
+    from dataclasses import replace
+
+    from oracle import oracle as O
+
+    pics = [_oracle_pic(f) for f in frames]
+    c = replace(_oracle_cfg(cfg), threads=threads)
+    packets = []
+    for p in pics:
+        k, msg, pkt = O.encode(c, p)
+        assert k == 0, msg
+        packets.append(pkt)
+
+    def enc():
+        for p in pics:
+            assert O.encode(c, p)[0] == 0
+
+    def dec():
+        for pkt in packets:
+            assert O.decode(pkt, 0, threads)[0] == 0
+
+    return len(pics) / _best(enc, reps), len(pics) / _best(dec, reps)
+
+
+def cpu_baseline(frames, cfg):
+    """Encode and decode rates of the CPU codec at every host thread and at
+    one, beside the crate's own published rates for comparison."""
+    import rivet_prores_b200 as P
+
+    cores = os.cpu_count()
+    n_all = min(4, len(frames))
+    enc_all, dec_all = cpu_codec_rates(frames[:n_all], cfg, 0, reps=5)
+    enc_1, dec_1 = cpu_codec_rates(frames[:1], cfg, 1, reps=5)
+    rt = 1.0 / (1.0 / enc_all + 1.0 / dec_all)
+    return {"value": round(rt, 3), "unit": "frames/s", "cores": cores, "kind": "port",
+            "encode_fps": round(enc_all, 3), "decode_fps": round(dec_all, 3),
+            "encode_fps_1_thread": round(enc_1, 3), "decode_fps_1_thread": round(dec_1, 3),
+            "sample": f"UHD 422 HQ frames: encode and decode timed separately, best of 5, pictures prepared "
+                      f"outside the timed region; {n_all} frames on all {cores} host threads, 1 frame on 1 thread; "
+                      f"`value` is the round trip (1 / (1/encode + 1/decode)) on all threads",
+            "code": "the oracle's scalar restatement of the crate's CPU path (no hand-written SIMD; the crate's "
+                    "SIMD levels give bit-identical output), compiled -O3 -march=x86-64-v3 -ffp-contract=off",
+            "published_crate": "README.md: 1920x1080 422 HQ 296 encode / 907 decode frames/s on 32 threads of a "
+                               "Ryzen 9 9950X, i.e. about 74 / 227 at UHD (4x the samples); other hardware"}
 
 
 def run_reference(args):
@@ -149,7 +221,7 @@ def run_reference(args):
     n = 2
     frames = workloads.uhd_422_hq(n, config=1, unique=n)
     cfg = O.Config(3)
-    pics = [O.Picture(f.width, f.height, f.bit_depth, 2, 0, (0, 0, 2, 2, 2), f.data, None) for f in frames]
+    pics = [_oracle_pic(f) for f in frames]
 
     def step():
         for p in pics:
@@ -181,13 +253,95 @@ def run_reference(args):
     }))
 
 
+# ---------------------------------------------------------------- GPU
+
+def time_jobs(enc, dec, stream, steps, warmup):
+    """Device times (ms, summed over `steps`) of the encode and the decode
+    job, each one CUDA-graph launch a step, with CUDA events on the
+    launching stream."""
+    import torch
+
+    for _ in range(warmup):
+        enc.launch(stream, graph=True)
+        dec.launch(stream, graph=True)
+    stream.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            ev[k][0].record(stream)
+            enc.launch(stream, graph=True)
+            ev[k][1].record(stream)
+            dec.launch(stream, graph=True)
+            ev[k][2].record(stream)
+    stream.synchronize()
+    t_enc = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(steps))
+    t_dec = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(steps))
+    return t_enc, t_dec, ev[0][0].elapsed_time(ev[-1][2])
+
+
+def check_exact(frames, configs, packets, planes):
+    """Every packet equals the oracle's encode of its frame, and every
+    decoded picture the oracle's decode of its packet."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    bad = []
+    for i, (f, c) in enumerate(zip(frames, configs)):
+        k, msg, want = O.encode(_oracle_cfg(c), _oracle_pic(f))
+        if k != 0 or bytes(packets[i]) != want:
+            bad.append(f"packet {i}")
+            continue
+        k, msg, pic = O.decode(want)
+        d = planes[i]
+        if k != 0 or not np.array_equal(d.data, pic.data) or (pic.alpha is not None and
+                                                            not np.array_equal(d.alpha, pic.alpha)):
+            bad.append(f"picture {i}")
+    return not bad, bad[:5]
+
+
+def run_config(name, batch, stream, steps, warmup, check, local):
+    """One benchmark configuration: its frames encoded in one graph-captured
+    launch and their packets decoded in another, each timed over `steps`
+    launches; throughput, algorithmic HBM GB/s and bit-exactness."""
+    import rivet_prores_b200 as P
+
+    frames = [f for f, _ in batch]
+    configs = [c for _, c in batch]
+    enc = P.EncodeJob(frames, configs, device=local)
+    enc.launch(stream)
+    packets = enc.fetch(stream)
+    assert all(isinstance(p, bytes) for p in packets), packets[:1]
+    dec = P.DecodeJob(packets, device=local)
+    dec.launch(stream)
+    planes = dec.fetch(stream)
+    t_enc, t_dec, _ = time_jobs(enc, dec, stream, steps, warmup)
+    n = len(frames)
+    samples = sum(int(f.data.size) + (0 if f.alpha is None else int(f.alpha.size)) for f in frames)
+    pkt_bytes = sum(len(p) for p in packets)
+    out = {"frames": n, "encode_fps": round(n * steps / (t_enc / 1000.0), 2),
+           "decode_fps": round(n * steps / (t_dec / 1000.0), 2),
+           "encode_ms": round(t_enc / steps, 4), "decode_ms": round(t_dec / steps, 4),
+           "algorithmic_bytes": 2 * samples + pkt_bytes,
+           "decode_hbm_gbs": round((2 * samples + pkt_bytes) / (t_dec / steps / 1000.0) / 1e9, 2),
+           "encode_hbm_gbs": round((2 * samples + pkt_bytes) / (t_enc / steps / 1000.0) / 1e9, 2),
+           "form": "one CUDA-graph launch per direction over the whole batch, resident buffers"}
+    if check:
+        out["bit_exact"], bad = check_exact(frames, configs, packets, planes)
+        if bad:
+            out["mismatches"] = bad
+    enc.close()
+    dec.close()
+    return name, out
+
+
 def run_b200(args):
     import numpy as np
     import torch
 
     import rivet_prores_b200 as P
     from rivet_prores_b200 import workloads
-    from rivet_prores_b200.sharding import max_over_ranks
+    from rivet_prores_b200.sharding import max_over_ranks, shard_by_macroblocks
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -202,7 +356,13 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     B = args.batch
-    frames = workloads.uhd_422_hq(B, config=1 + rank, unique=args.unique)
+    # This rank's share of a global batch of B x world frames, split as the
+    # library's multi-device calls split one (all frames are UHD, so the
+    # shares are equal).
+    mine = shard_by_macroblocks([(W, H)] * (B * world), world)[rank]
+    unique = args.unique or B
+    distinct = workloads.uhd_422_hq_at(mine[:unique])
+    frames = [distinct[k % len(distinct)] for k in range(B)]
     cfg = P.Config(P.Profile.Hq)
     stream = torch.cuda.Stream()
 
@@ -225,30 +385,14 @@ def run_b200(args):
     packets = enc.fetch(stream)
     assert all(isinstance(p, bytes) for p in packets), packets[:1]
     dec = P.DecodeJob(packets, device=local)
-
-    # Bit-exactness on the GPU: the first frame's packet and picture equal
-    # the oracle's.
-    exact = None
-    if rank == 0:
-        from oracle import oracle as O
-
-        f0 = frames[0]
-        k, msg, want = O.encode(O.Config(3), O.Picture(W, H, 10, 2, 0, (0, 0, 2, 2, 2), f0.data, None))
-        dec.launch(stream)
-        got = dec.fetch(stream)[0]
-        k2, msg2, pic = O.decode(want)
-        exact = bool(k == 0 and packets[0] == want and np.array_equal(got.data, pic.data))
-        if not exact:
-            print(json.dumps({"error": "GPU output differs from the oracle"}), file=sys.stderr)
-
-    def step():
-        enc.launch(stream, graph=True)
-        dec.launch(stream, graph=True)
+    dec.launch(stream)
+    first_planes = dec.fetch(stream)
+    pkt_bytes = sum(len(p) for p in packets)
 
     for _ in range(args.warmup):
-        step()
+        enc.launch(stream, graph=True)
+        dec.launch(stream, graph=True)
     stream.synchronize()
-
     uuid = str(getattr(torch.cuda.get_device_properties(local), "uuid", ""))
     clocks = Clocks(uuid)
     if dist:
@@ -256,33 +400,22 @@ def run_b200(args):
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.4)
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            ev[k][0].record(stream)
-            enc.launch(stream, graph=True)
-            ev[k][1].record(stream)
-            dec.launch(stream, graph=True)
-            ev[k][2].record(stream)
-    stream.synchronize()
+    t_enc, t_dec, total = time_jobs(enc, dec, stream, args.steps, 0)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
-    t_enc = sum(ev[k][0].elapsed_time(ev[k][1]) for k in range(args.steps))
-    t_dec = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(args.steps))
-    total = ev[0][0].elapsed_time(ev[-1][2])
     total, t_enc, t_dec = max_over_ranks([total, t_enc, t_dec], dist, "cuda")
     frames_done = B * args.steps * world
     value = frames_done / (total / 1000.0)
     dec_fps = frames_done / (t_dec / 1000.0)
     enc_fps = frames_done / (t_enc / 1000.0)
+    ms_per_step = total / args.steps
 
-    # Per-kernel device times (a separate, profiled launch of each job: the
+    # Per-kernel device times: a separate, profiled launch of each job (the
     # kernels bracketed by events on the launching stream).
     os.environ["PRORES_PROFILE_KERNELS"] = "1"
     penc = P.EncodeJob(frames, cfg, device=local)
     pdec = P.DecodeJob(packets, device=local)
-    kernel_ms = {}
-    counts = {}
+    kernel_ms, counts = {}, {}
     for job in (penc, pdec):
         job.launch(stream)
         stream.synchronize()
@@ -296,10 +429,37 @@ def run_b200(args):
     penc.close()
     pdec.close()
     launches_per_step = sum(counts.values())
-    dominant = max(kernel_ms, key=kernel_ms.get)
-    dom_avg = kernel_ms[dominant] / counts[dominant]
     peak, peak_kind = load_peaks()
-    achieved = ALGO_BYTES_PER_FRAME * B / (dom_avg / 1000.0) / 1e9
+    p_frame = pkt_bytes / B
+    kernels = {}
+    for name, ms in sorted(kernel_ms.items(), key=lambda x: -x[1]):
+        entry = {"ms_per_step": round(ms, 4), "launches": counts[name]}
+        if name in KERNEL_BYTES:
+            fn, basis = KERNEL_BYTES[name]
+            per_launch = fn(SAMPLES, p_frame) * B
+            gbs = per_launch / (ms / counts[name] / 1000.0) / 1e9
+            entry.update({"algorithmic_bytes_per_launch": int(per_launch), "basis": basis,
+                          "achieved_gbs": round(gbs, 2), "frac": round(gbs / peak, 4)})
+        kernels[name] = entry
+    dominant = max(kernel_ms, key=kernel_ms.get)
+    dom = kernels[dominant]
+    step_bytes = 2 * (p_frame + 2 * SAMPLES) * B
+    step_gbs = step_bytes / (ms_per_step / 1000.0) / 1e9
+    cap = CAPTURED.get(dominant)
+    roofline = {
+        "kernel": dominant, "bound": "hbm", "achieved": dom.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
+        "frac": dom.get("frac"), "peak_source": f"{peak_kind} (HBM copy bandwidth)",
+        "algorithmic_bytes_per_launch": dom.get("algorithmic_bytes_per_launch"), "basis": dom.get("basis"),
+        "launch_ms": round(kernel_ms[dominant] / counts[dominant], 4), "launches_per_step": counts[dominant],
+        "arithmetic": "achieved = algorithmic_bytes_per_launch / launch_ms; frac = achieved / peak",
+        "traffic": round(cap["dram_bytes_per_frame"] * B) if cap else None,
+        "traffic_source": (cap["capture"] + ", scaled to this launch's frames; not measured by this run")
+        if cap else "no capture of this kernel",
+        "issue_active_pct": cap["issue_active_pct"] if cap else None,
+        "step": {"bytes": int(step_bytes), "basis": "packet + u16 planes, each direction, every frame",
+                 "ms": round(ms_per_step, 4), "achieved_gbs": round(step_gbs, 2),
+                 "frac": round(step_gbs / peak, 4)},
+    }
 
     # Plain: one frame per launch, no graph, each frame waited for.
     plain_n = min(B, 8)
@@ -342,26 +502,40 @@ def run_b200(args):
         t = time_round_trip(pipe, e2e_steps, warmup=2) * e2e_steps
         h2d, d2h = pipe.bytes_per_step()
         t = max_over_ranks([t], dist, "cuda")[0]
-        e2e = {"value": round(B * e2e_steps * world / (t / 1000.0), 3), "unit": "frames/s",
+        sec = t / 1000.0
+        e2e = {"value": round(B * e2e_steps * world / sec, 3), "unit": "frames/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+               "pcie_gbs_each_way": {"h2d": round(h2d * e2e_steps / sec / 1e9, 2),
+                                     "d2h": round(d2h * e2e_steps / sec / 1e9, 2)},
                "path": f"stream.RoundTripPipeline: prores_{{encode,decode}}_job_{{upload,launch,fetch}}, pinned host "
                        f"buffers, {len(pipe.parts)} parts on their own streams"}
         assert [bytes(p) for p in pipe.packets] == packets
-        assert np.array_equal(pipe.planes[0], dec.fetch(stream)[0].data)
+        assert np.array_equal(pipe.planes[0], first_planes[0].data)
         pipe.close()
+
+    # Bit-exactness on the GPU: every frame of the first step, packet and
+    # picture, against the oracle.
+    exact, mismatches = None, []
+    if rank == 0 and not args.no_check:
+        exact, mismatches = check_exact(frames[:unique], [cfg] * unique, packets, first_planes)
+        if not exact:
+            print(json.dumps({"error": "GPU output differs from the oracle", "where": mismatches}), file=sys.stderr)
+
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = {}
+        for name, make in [("config1_1080p_hq_x64", lambda: workloads.hd_422_hq(64)),
+                           ("config2_uhd_4444xq_alpha_x16", lambda: workloads.uhd_4444xq_alpha(16)),
+                           ("config3_mixed_x96", lambda: workloads.mixed_batch(96))]:
+            key, res = run_config(name, make(), stream, steps=5, warmup=3, check=not args.no_check, local=local)
+            configs[key] = res
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        from oracle import oracle as O
-
-        n_cpu = min(8, args.unique)
-        fps, cores = cpu_baseline(frames[:n_cpu], O.Config(3))
-        cpu = {"value": round(fps, 3), "unit": "frames/s", "cores": cores, "kind": "port",
-               "sample": f"{n_cpu} UHD 422 HQ frames, encode + decode each, best of 3, oracle codec on "
-                         f"{cores} threads"}
+        cpu = cpu_baseline(frames, cfg)
 
     serve = None
-    if rank == 0 and args.serve_seconds > 0:
+    if rank == 0 and world == 1 and args.serve_seconds > 0:
         serve = run_serving(args, local)
 
     if dist:
@@ -371,32 +545,27 @@ def run_b200(args):
         return
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(total / args.steps, 4), "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded PCG64 cosines + rectangles + noise, rivet_prores_b200/workloads.py)",
-        "config": {"workload": "uhd_422hq_transcode", "frames_per_step": B, "width": W, "height": H,
-                   "chroma": "4:2:2", "bit_depth": 10, "profile": "HQ (apch)", "target_frame_bytes": 3_643_238,
+        "config": {"workload": "uhd_422hq_transcode", "frames_per_step": B, "distinct_pictures": unique,
+                   "width": W, "height": H, "chroma": "4:2:2", "bit_depth": 10, "profile": "HQ (apch)",
+                   "target_frame_bytes": TARGET,
                    "step": "encode B frames, then decode their packets; one graph launch each, resident buffers",
                    "l2": "inputs larger than L2 (B x 33 MB of planes per step)",
-                   "parallelism": f"{world} rank(s), frames sharded by rank, no collective",
+                   "parallelism": f"{world} rank(s), frames split by macroblock count, no collective",
                    "tuning": tuning, "tuning_source": tuning_note},
-        "bit_exact": exact,
+        "bit_exact": exact, "bit_exact_scope": f"all {unique} packets and pictures of the first step vs the oracle",
         "decode_fps": round(dec_fps, 3), "encode_fps": round(enc_fps, 3),
         "plain": {"value": round(plain_fps, 3), "decode_fps": round(plain_dec_fps, 3),
                   "encode_fps": round(plain_enc_fps, 3), "frames": plain_n,
                   "form": "one frame per launch, no graph, waited for"},
         "e2e": e2e,
         "gpu_launches": launches_per_step * args.steps,
-        "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(kernel_ms.items(), key=lambda x: -x[1])},
-        "roofline": {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": (round(PROFILED[dominant]["dram_bytes_per_frame"] * B) if dominant in PROFILED
-                                 else None),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, 14 frames, "
-                                       "scaled to the launch's frames (profiles/kernels_uhd_422hq_b14.md)",
-                     "issue_active_pct": PROFILED.get(dominant, {}).get("issue_active_pct"),
-                     "peak_source": peak_kind,
-                     "algorithmic_bytes": f"{ALGO_BYTES_PER_FRAME} B per frame (packet + u16 planes) x {B}"},
+        "kernels_ms_per_step": {k: v["ms_per_step"] for k, v in kernels.items()},
+        "kernels": kernels,
+        "roofline": roofline,
+        "configs": configs,
         "cpu_baseline": cpu,
         "serve": serve,
         "clocks": clock_info,
@@ -406,10 +575,10 @@ def run_b200(args):
 
 def run_serving(args, device):
     """Poisson requests (70 % decode, 30 % encode) over the heterogeneous
-    mix, served with continuous batching under an 8 GiB device budget, at
-    the offered rate (near what the server can take: throughput) and at half
-    of it (latency with headroom); then the full offered load served one
-    request per launch."""
+    mix, served with continuous batching under an 8 GiB device budget: at
+    the offered rate for the full run (with p50/p99 per 10 s window, to show
+    whether the queue is stationary), at half the rate, and the offered
+    load served one request per launch."""
     import numpy as np
 
     import rivet_prores_b200 as P
@@ -437,12 +606,11 @@ def run_serving(args, device):
            "budget_bytes": 8 << 30,
            "host_buffers": "requests (packets, frames) in page-locked receive buffers; decoded planes into "
                            "pooled page-locked buffers"}
-    # Batches of at most 16: large enough to fill the device, small enough
-    # that a request does not wait behind a long batch.
+    window = 10.0
     for name, workers, max_batch, seconds, rate in [
             ("batched", 4, 16, args.serve_seconds, args.serve_rate),
-            ("batched_half_load", 4, 16, max(1.0, args.serve_seconds / 2), args.serve_rate / 2),
-            ("plain", 1, 1, max(1.0, args.serve_seconds / 4), args.serve_rate)]:
+            ("batched_half_load", 4, 16, max(1.0, min(20.0, args.serve_seconds / 2)), args.serve_rate / 2),
+            ("plain", 1, 1, max(1.0, min(10.0, args.serve_seconds / 6)), args.serve_rate)]:
         # One backend (and its pool of page-locked output buffers) for the
         # warm-up and the measured run.
         backend = S.GpuBackend(device)
@@ -450,7 +618,7 @@ def run_serving(args, device):
         S.poisson_run(srv, maker(1), rate=200.0, seconds=0.3)  # workspaces allocated, not measured
         srv.close()
         srv = S.Server(backend, memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
-        st = S.poisson_run(srv, maker(2), rate=rate, seconds=seconds)
+        st = S.poisson_run(srv, maker(2), rate=rate, seconds=seconds, window=window)
         srv.close()
         out[name] = st
     return out

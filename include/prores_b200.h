@@ -114,6 +114,17 @@ typedef struct prores_frame_header {
 prores_ctx *prores_create(int device);
 void prores_destroy(prores_ctx *ctx);
 
+/* Bound, in ms, on every wait of the host for the device in calls made on
+ * ctx from now on (0: no bound; default 60000). A call whose wait runs out
+ * returns PRORES_TIMEOUT and leaves its device work running: a job stays
+ * valid (its fetch can be called again), and a one-shot call's device
+ * buffers are reused only after that work has finished. No reference
+ * counterpart: the crate never waits on a device; this keeps its promise
+ * that every failure comes back as an error (src/error.rs:3-5) when a
+ * device stops making progress. */
+int prores_set_timeout(prores_ctx *ctx, uint32_t ms);
+uint32_t prores_get_timeout(prores_ctx *ctx);
+
 /* Message of the last failing call made on this thread, formatted like the
  * crate's Error Display ("invalid ProRes data: ..."). */
 const char *prores_last_error(void);
@@ -164,6 +175,30 @@ int prores_encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
                         prores_buf *out, int *status);
 
 void prores_buffer_free(void *p);
+
+/* ---- one batch over several devices ------------------------------------ */
+
+/* The frame-to-device split the *_multi calls use: part[i] in [0, parts)
+ * for frame i of width[i] x height[i]. Largest frames first, each to the
+ * part with the fewest macroblocks so far (ties to the lower part). No
+ * reference counterpart: the crate leaves frame-level parallelism to its
+ * caller (src/decode.rs:15-17, src/pool.rs:3-8); this is that caller's
+ * split, done once for every user. Host only, no device needed. */
+int prores_shard_frames(const uint32_t *width, const uint32_t *height, int n, int parts, int *part);
+
+/* prores_decode_batch over several devices: ctxs[0..n_ctx) are contexts
+ * (normally one per GPU). The frames are split by prores_shard_frames on
+ * their headers' sizes, each context decodes its share in one batched call
+ * on a host thread of its own, and out[i], status[i] and
+ * prores_batch_error(i) come back in input order as from one call. The
+ * devices exchange nothing: frames are independent. */
+int prores_decode_batch_multi(prores_ctx *const *ctxs, int n_ctx, const prores_buf *in, int n,
+                              uint32_t out_bit_depth, prores_frame *out, int *status);
+
+/* prores_encode_batch over several devices, split and gathered the same
+ * way; out[i] are library-allocated packets (prores_buffer_free). */
+int prores_encode_batch_multi(prores_ctx *const *ctxs, int n_ctx, const prores_config *cfg, const prores_frame *in,
+                              int n, prores_buf *out, int *status);
 
 /* ---- frames found in a MOV, frames in device memory -------------------- */
 

@@ -387,6 +387,17 @@ class Context:
         t = tuning._c()
         _check(_abi.lib().prores_set_tuning(self.handle, ctypes.byref(t)))
 
+    @property
+    def timeout_ms(self) -> int:
+        """Bound on every host wait for the device in this context's calls
+        (0: none). A call whose wait runs out raises Error.Timeout and leaves
+        its device work running; a job stays usable."""
+        return int(_abi.lib().prores_get_timeout(self.handle))
+
+    @timeout_ms.setter
+    def timeout_ms(self, ms: int) -> None:
+        _check(_abi.lib().prores_set_timeout(self.handle, int(ms)))
+
     def __del__(self):
         h = getattr(self, "handle", None)
         lib = getattr(_abi, "_lib", None) if _abi is not None else None
@@ -447,11 +458,14 @@ class Decoder:
             raise r
         return r
 
-    def decode_batch(self, datas: Sequence[bytes], alloc=None) -> List[Union[Frame, Error]]:
+    def decode_batch(self, datas: Sequence[bytes], alloc=None, devices: Optional[Sequence[int]] = None
+                     ) -> List[Union[Frame, Error]]:
         """Decodes every frame in one batched launch; each entry is a Frame or
         the Error that frame gave. `alloc(n, dtype)`, when given, makes the
         output arrays (for example from a pool of page-locked buffers, which
-        the planes then reach by DMA with no host copy)."""
+        the planes then reach by DMA with no host copy). With `devices`, the
+        batch is split over those GPUs by macroblock count (one batched call
+        each, on host threads of their own) and gathered in input order."""
         L = _abi.lib()
         n = len(datas)
         alloc = alloc or np.empty
@@ -475,7 +489,11 @@ class Decoder:
                 if alpha is not None:
                     outs[i].alpha, outs[i].alpha_len = _ptr16(alpha), info.alpha_len
                 arrays[i] = (data, alpha)
-        code = L.prores_decode_batch(context(self.device).handle, bufs, n, depth, outs, status)
+        if devices:
+            ctxs = (ctypes.c_void_p * len(devices))(*[context(d).handle for d in devices])
+            code = L.prores_decode_batch_multi(ctxs, len(devices), bufs, n, depth, outs, status)
+        else:
+            code = L.prores_decode_batch(context(self.device).handle, bufs, n, depth, outs, status)
         if code != _abi.OK:
             raise _error(code)
         for i in range(n):
@@ -636,10 +654,11 @@ class Encoder:
             raise r
         return r
 
-    def encode_batch(self, frames: Sequence[Frame], configs: Optional[Sequence[Config]] = None
-                     ) -> List[Union[bytes, Error]]:
+    def encode_batch(self, frames: Sequence[Frame], configs: Optional[Sequence[Config]] = None,
+                     devices: Optional[Sequence[int]] = None) -> List[Union[bytes, Error]]:
         """Encodes every frame (each with its own Config, default this
-        encoder's) in one batched launch."""
+        encoder's) in one batched launch; with `devices`, split over those
+        GPUs by macroblock count and gathered in input order."""
         L = _abi.lib()
         n = len(frames)
         configs = list(configs) if configs is not None else [self._config] * n
@@ -651,7 +670,11 @@ class Encoder:
         for i in range(n):
             cfgs[i] = configs[i]._c()
             ins[i] = _frame_to_c(frames[i], keep)
-        code = L.prores_encode_batch(context(self.device).handle, cfgs, ins, n, outs, status)
+        if devices:
+            ctxs = (ctypes.c_void_p * len(devices))(*[context(d).handle for d in devices])
+            code = L.prores_encode_batch_multi(ctxs, len(devices), cfgs, ins, n, outs, status)
+        else:
+            code = L.prores_encode_batch(context(self.device).handle, cfgs, ins, n, outs, status)
         if code != _abi.OK:
             raise _error(code)
         res: List[Union[bytes, Error]] = []

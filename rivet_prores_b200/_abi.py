@@ -158,6 +158,14 @@ def lib():
                                                 vp]),
         "prores_set_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
         "prores_get_tuning": (ctypes.c_int, [vp, P(Tuning_)]),
+        "prores_set_timeout": (ctypes.c_int, [vp, ctypes.c_uint32]),
+        "prores_shard_frames": (ctypes.c_int, [P(ctypes.c_uint32), P(ctypes.c_uint32), ctypes.c_int, ctypes.c_int,
+                                               P(ctypes.c_int)]),
+        "prores_decode_batch_multi": (ctypes.c_int, [P(vp), ctypes.c_int, P(Buf_), ctypes.c_int, ctypes.c_uint32,
+                                                     P(Frame_), P(ctypes.c_int)]),
+        "prores_encode_batch_multi": (ctypes.c_int, [P(vp), ctypes.c_int, P(Config_), P(Frame_), ctypes.c_int,
+                                                     P(Buf_), P(ctypes.c_int)]),
+        "prores_get_timeout": (ctypes.c_uint32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

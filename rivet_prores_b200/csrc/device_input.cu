@@ -171,7 +171,10 @@ struct DeviceHeads {
             PR_CUDA(cudaMemcpyAsync(host + at[i], d_data + frames[i].offset + p, l, cudaMemcpyDeviceToHost, s),
                     "header fetch");
         }
-        PR_CUDA(cudaStreamSynchronize(s), "header fetch");
+        {
+            Status w = wait_stream(s, ws.wait_ms, "header fetch");
+            if (w) return w;
+        }
         for (int i = 0; i < n; i++)
             if (at[i] != SIZE_MAX) keep(i, host + at[i], len[i]);
         return Status();
@@ -233,7 +236,7 @@ int prores_scan_frames_device(prores_ctx *ctx, const uint8_t *d_data, size_t len
         uint8_t *host = static_cast<uint8_t *>(ws->host_small.p);
         unsigned int found = 0;
         st = cuda_status(cudaMemcpyAsync(host, counter, sizeof found, cudaMemcpyDeviceToHost, s), "scan");
-        if (!st) st = cuda_status(cudaStreamSynchronize(s), "scan");
+        if (!st) st = wait_stream(s, ws->wait_ms, "scan");
         if (st) break;
         memcpy(&found, host, sizeof found);
         if (found > room) {  // more candidates than room: once more with room for all
@@ -245,7 +248,7 @@ int prores_scan_frames_device(prores_ctx *ctx, const uint8_t *d_data, size_t len
             if (!st)
                 st = cuda_status(cudaMemcpyAsync(host + 8ull * found, size, 4ull * found, cudaMemcpyDeviceToHost, s),
                                  "scan");
-            if (!st) st = cuda_status(cudaStreamSynchronize(s), "scan");
+            if (!st) st = wait_stream(s, ws->wait_ms, "scan");
             if (st) break;
             cand.resize(found);
             for (unsigned int k = 0; k < found; k++) {
@@ -256,7 +259,7 @@ int prores_scan_frames_device(prores_ctx *ctx, const uint8_t *d_data, size_t len
         *count = resolve(cand, len, frames, cap);
         break;
     }
-    ctx->impl.release(std::move(ws));
+    ctx->impl.release_or_retire(std::move(ws));
     return st ? fail_status(st) : PRORES_OK;
 }
 
@@ -271,7 +274,7 @@ int prores_probe_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len,
     if (!ws) return fail_status(make_status(PRORES_DEVICE, "no stream"));
     DeviceHeads heads;
     st = heads.fetch(*ws, d_data, frames, n, ws->stream);
-    ctx->impl.release(std::move(ws));
+    ctx->impl.release_or_retire(std::move(ws));
     if (st) return fail_status(st);
     std::vector<Status> errs(n);
     for (int i = 0; i < n; i++) {
@@ -320,8 +323,7 @@ int prores_decode_device(prores_ctx *ctx, const uint8_t *d_data, size_t data_len
     Status first;
     if (!st) st = fetch_decode(*ws, plan, s, out, status, &first, true);
     if (st) {
-        cudaStreamSynchronize(s);
-        ctx->impl.release(std::move(ws));
+        ctx->impl.release_or_retire(std::move(ws));
         return fail_status(st);
     }
     ctx->impl.release(std::move(ws));

@@ -447,7 +447,10 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
             PR_CUDA(cudaMemcpyAsync(sizes, ws.enc_alpha_bytes.p, 8 * nf, cudaMemcpyDeviceToHost, s), "size download");
             PR_CUDA(cudaMemcpyAsync(flags, ws.enc_alpha_bits.p, 4 * nf, cudaMemcpyDeviceToHost, s), "size download");
         }
-        PR_CUDA(cudaStreamSynchronize(s), "encode");
+        {
+            Status w = wait_stream(s, ws.wait_ms, "encode");
+            if (w) return w;
+        }
         std::copy(sizes, sizes + nf, plan.frame_size.begin());
         std::copy(flags, flags + nf, plan.frame_status.begin());
         bool over = false;
@@ -484,7 +487,10 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
                 "packet download");
         pos += plan.frame_size[f];
     }
-    PR_CUDA(cudaStreamSynchronize(s), "encode");
+    {
+        Status w = wait_stream(s, ws.wait_ms, "encode");
+        if (w) return w;
+    }
     out.assign(plan.frames.size(), prores_buf{nullptr, 0});
     pos = 0;
     std::vector<Status> errs(plan.frames.size());
@@ -540,8 +546,7 @@ static int encode_batch(prores_ctx *ctx, const prores_config *cfg, const prores_
     Status first;
     if (!st) st = fetch_encode(ctx->impl, *ws, *plan, s, packets, status, &first);
     if (st) {
-        cudaStreamSynchronize(s);
-        ctx->impl.release(std::move(ws));
+        ctx->impl.release_or_retire(std::move(ws));
         return efail(st);
     }
     // The packets lie in the workspace's staging buffer: copied out before
@@ -601,7 +606,7 @@ int prores_encode_job_create(prores_ctx *ctx, const prores_config *cfg, const pr
         if (!j->ws) st = make_status(PRORES_DEVICE, "no stream");
     }
     if (!st) st = upload_encode(ctx->impl, *j->ws, *j->plan, in, j->ws->stream, true, false);
-    if (!st) st = cuda_status(cudaStreamSynchronize(j->ws->stream), "upload");
+    if (!st) st = wait_stream(j->ws->stream, j->ws->wait_ms, "upload");
     if (st) {
         prores_encode_job_destroy(j);
         return efail(st);
@@ -620,6 +625,7 @@ int prores_encode_job_upload(prores_encode_job *job, const prores_frame *in, int
             return efail(make_status(PRORES_CONFIG, "a job's frame formats are fixed"));
     }
     cudaSetDevice(job->ctx->impl.device);
+    job->ctx->impl.refresh(*job->ws);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
     Status st = upload_encode(job->ctx->impl, *job->ws, *job->plan, in, s, false, false);
     return st ? efail(st) : PRORES_OK;
@@ -657,6 +663,7 @@ int prores_encode_job_launch(prores_encode_job *job, void *stream, int use_graph
 
 int prores_encode_job_fetch(prores_encode_job *job, void *stream, prores_buf *out, int *status) {
     cudaSetDevice(job->ctx->impl.device);
+    job->ctx->impl.refresh(*job->ws);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
     Status first;
     Status st = fetch_encode(job->ctx->impl, *job->ws, *job->plan, s, job->packets, status, &first);
@@ -671,9 +678,12 @@ void prores_encode_job_destroy(prores_encode_job *job) {
     cudaSetDevice(job->ctx->impl.device);
     for (auto e : job->kt.events) cudaEventDestroy(e);
     if (job->ws) {
-        cudaStreamSynchronize(job->ws->stream);
+        // Its work may still run (a fetch that timed out): the workspace and
+        // graph are then kept until it is done.
+        cudaGraphExec_t graph = job->plan ? job->plan->graph : nullptr;
+        if (job->plan) job->plan->graph = nullptr;
         job->plan.reset();
-        job->ctx->impl.release(std::move(job->ws));
+        job->ctx->impl.release_or_retire(std::move(job->ws), graph);
     }
     delete job;
 }

@@ -10,7 +10,11 @@
 
 #include "engine.h"
 
+#include <sched.h>
+#include <time.h>
+
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -28,6 +32,10 @@ static thread_local std::vector<std::string> g_batch_errors;
 
 void set_last_error(const Status &s) { g_last_error = display(s); }
 
+void set_last_error_text(const std::string &text) { g_last_error = text; }
+
+void set_batch_error_texts(const std::vector<std::string> &texts) { g_batch_errors = texts; }
+
 void set_batch_errors(const std::vector<Status> &errs) {
     g_batch_errors.assign(errs.size(), std::string());
     for (size_t i = 0; i < errs.size(); i++)
@@ -36,7 +44,40 @@ void set_batch_errors(const std::vector<Status> &errs) {
 
 Status cuda_status(cudaError_t e, const char *what) {
     if (e == cudaSuccess) return Status();
+    // Only the bounded waits below report "not ready" up to here.
+    if (e == cudaErrorNotReady)
+        return make_status(PRORES_TIMEOUT, strf("%s: the device did not finish within the wait limit", what));
     return make_status(PRORES_DEVICE, strf("%s: %s", what, cudaGetErrorString(e)));
+}
+
+cudaError_t wait_event(cudaEvent_t e, uint32_t limit_ms) {
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q != cudaErrorNotReady) return q;
+        const double us = std::chrono::duration<double, std::micro>(clock::now() - t0).count();
+        if (limit_ms && us >= 1000.0 * limit_ms) return cudaErrorNotReady;
+        // Short waits (most of them) are polled; a long one sleeps between
+        // polls, a little longer the longer it has waited.
+        if (us < 2000.0) {
+            sched_yield();
+        } else {
+            const long ns = us < 20000.0 ? 20000L : 100000L;
+            timespec ts{0, ns};
+            nanosleep(&ts, nullptr);
+        }
+    }
+}
+
+Status wait_stream(cudaStream_t s, uint32_t limit_ms, const char *what) {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    if (r != cudaSuccess) return cuda_status(r, what);
+    r = cudaEventRecord(e, s);
+    if (r == cudaSuccess) r = wait_event(e, limit_ms);
+    cudaEventDestroy(e);
+    return cuda_status(r, what);
 }
 
 #define PR_CUDA(expr, what)                                   \
@@ -62,7 +103,16 @@ cudaError_t DeviceBuf::reserve(size_t bytes) {
     cap = 0;
     cudaError_t e = cudaMallocAsync(&p, want, stream);
     // Usable from any stream once the workspace's stream has passed it.
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess) {
+        cudaEvent_t ev;
+        e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) {
+            e = cudaEventRecord(ev, stream);
+            if (e == cudaSuccess) e = wait_event(ev, wait_ms);
+            cudaEventDestroy(ev);
+        }
+        if (e == cudaErrorNotReady) return e;  // the allocation stands; the caller's workspace is retired
+    }
     if (e != cudaSuccess) {
         p = nullptr;
         return e;
@@ -117,7 +167,7 @@ cudaError_t Stager::slot(int &i) {
     }
     i = (int)(issued % kSlots);
     if (issued >= (uint64_t)kSlots) {
-        cudaError_t e = cudaEventSynchronize(ev[i]);
+        cudaError_t e = wait_event(ev[i], wait_ms);
         if (e != cudaSuccess) return e;
         if (pend[i].dst) memcpy(pend[i].dst, static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk, pend[i].len);
     }
@@ -163,12 +213,16 @@ cudaError_t Stager::d2h(void *dst, const void *src, size_t len, cudaStream_t s) 
     return cudaSuccess;
 }
 
+void Stager::forget() {
+    for (auto &p : pend) p = Pending{};
+}
+
 cudaError_t Stager::finish() {
     const uint64_t first = issued > (uint64_t)kSlots ? issued - kSlots : 0;
     for (uint64_t k = first; k < issued; k++) {
         const int i = (int)(k % kSlots);
         if (!pend[i].dst) continue;
-        cudaError_t e = cudaEventSynchronize(ev[i]);
+        cudaError_t e = wait_event(ev[i], wait_ms);
         if (e != cudaSuccess) return e;
         memcpy(pend[i].dst, static_cast<uint8_t *>(buf.p) + (size_t)i * kChunk, pend[i].len);
         pend[i] = Pending{};
@@ -179,8 +233,10 @@ cudaError_t Stager::finish() {
 void Workspace::bind_stream() {
     for (DeviceBuf *b : {&bits, &frames, &pics, &slices, &slot_status, &pic_status, &coef, &coef_count, &planes,
                          &alpha, &weights, &counter, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost, &enc_pic_state,
-                         &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes, &enc_frame_out})
+                         &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes, &enc_frame_out}) {
         b->stream = stream;
+        b->wait_ms = wait_ms;
+    }
 }
 
 Workspace::~Workspace() {
@@ -188,16 +244,32 @@ Workspace::~Workspace() {
 }
 
 std::unique_ptr<Workspace> Context::acquire() {
+    uint32_t limit;
     {
         std::lock_guard<std::mutex> g(m);
+        limit = wait_ms;
+        // Retired workspaces whose work has finished go back to the pool.
+        for (size_t i = 0; i < retired.size();) {
+            if (cudaStreamQuery(retired[i].ws->stream) == cudaSuccess) {
+                if (retired[i].graph) cudaGraphExecDestroy(retired[i].graph);
+                free_ws.push_back(std::move(retired[i].ws));
+                retired.erase(retired.begin() + (long)i);
+            } else {
+                cudaGetLastError();
+                i++;
+            }
+        }
         if (!free_ws.empty()) {
             auto ws = std::move(free_ws.back());
             free_ws.pop_back();
+            ws->wait_ms = ws->stager.wait_ms = limit;
+            ws->bind_stream();
             return ws;
         }
     }
     auto ws = std::make_unique<Workspace>();
     ws->device = device;
+    ws->wait_ms = ws->stager.wait_ms = limit;
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
     ws->bind_stream();
@@ -206,8 +278,33 @@ std::unique_ptr<Workspace> Context::acquire() {
 
 void Context::release(std::unique_ptr<Workspace> ws) {
     if (!ws) return;
+    ws->stager.forget();
     std::lock_guard<std::mutex> g(m);
     free_ws.push_back(std::move(ws));
+}
+
+void Context::refresh(Workspace &ws) {
+    uint32_t limit;
+    {
+        std::lock_guard<std::mutex> g(m);
+        limit = wait_ms;
+    }
+    ws.wait_ms = ws.stager.wait_ms = limit;
+    ws.bind_stream();
+}
+
+void Context::release_or_retire(std::unique_ptr<Workspace> ws, cudaGraphExec_t graph) {
+    if (!ws) return;
+    const cudaError_t q = cudaStreamQuery(ws->stream);
+    if (q == cudaSuccess) {
+        if (graph) cudaGraphExecDestroy(graph);
+        release(std::move(ws));
+        return;
+    }
+    cudaGetLastError();
+    ws->stager.forget();
+    std::lock_guard<std::mutex> g(m);
+    retired.push_back(Retired{std::move(ws), graph});
 }
 
 Tuning Context::current_tuning() {
@@ -223,6 +320,11 @@ EntropyShape Context::current_entropy() {
 Context::~Context() {
     cudaSetDevice(device);
     free_ws.clear();
+    for (auto &r : retired) {
+        cudaStreamSynchronize(r.ws->stream);
+        if (r.graph) cudaGraphExecDestroy(r.graph);
+    }
+    retired.clear();
     if (tables.run_decode) cudaFree(tables.run_decode);
     if (tables.level_decode) cudaFree(tables.level_decode);
     if (tables.basis) cudaFree(tables.basis);
@@ -517,7 +619,10 @@ Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prore
         const uint16_t *src = (r.alpha ? ws.alpha.as<uint16_t>() : ws.planes.as<uint16_t>()) + r.src;
         PR_CUDA(ws.stager.d2h(r.dst, src, 2 * r.len, s), "plane download");
     }
-    PR_CUDA(cudaStreamSynchronize(s), "decode");
+    {
+        Status w = wait_stream(s, ws.wait_ms, "decode");
+        if (w) return w;
+    }
     PR_CUDA(ws.stager.finish(), "plane download");
     std::vector<Status> errs(n);
     for (int i = 0; i < n; i++) {
@@ -695,6 +800,19 @@ int prores_get_tuning(prores_ctx *ctx, prores_tuning *t) {
     return PRORES_OK;
 }
 
+int prores_set_timeout(prores_ctx *ctx, uint32_t ms) {
+    if (!ctx) return fail(make_status(PRORES_CONFIG, "no context"));
+    std::lock_guard<std::mutex> g(ctx->impl.m);
+    ctx->impl.wait_ms = ms;
+    return PRORES_OK;
+}
+
+uint32_t prores_get_timeout(prores_ctx *ctx) {
+    if (!ctx) return 0;
+    std::lock_guard<std::mutex> g(ctx->impl.m);
+    return ctx->impl.wait_ms;
+}
+
 void prores_destroy(prores_ctx *ctx) { delete ctx; }
 
 const char *prores_last_error(void) { return g_last_error.c_str(); }
@@ -750,8 +868,7 @@ int prores_decode_batch(prores_ctx *ctx, const prores_buf *in, int n, uint32_t o
     Status first;
     if (!st) st = fetch_decode(*ws, plan, s, out, status, &first);
     if (st) {
-        cudaStreamSynchronize(s);
-        ctx->impl.release(std::move(ws));
+        ctx->impl.release_or_retire(std::move(ws));
         return fail(st);
     }
     ctx->impl.release(std::move(ws));
@@ -808,7 +925,7 @@ int prores_decode_job_create(prores_ctx *ctx, const prores_buf *in, int n, uint3
     }
     if (!st) st = upload_decode(ctx->impl, *j->ws, j->plan, j->ws->stream);
     if (!st) st = upload_decode_bits(*j->ws, j->plan, in, j->ws->stream);
-    if (!st) st = cuda_status(cudaStreamSynchronize(j->ws->stream), "upload");
+    if (!st) st = wait_stream(j->ws->stream, j->ws->wait_ms, "upload");
     if (st) {
         prores_decode_job_destroy(j);
         return fail(st);
@@ -820,6 +937,7 @@ int prores_decode_job_create(prores_ctx *ctx, const prores_buf *in, int n, uint3
 int prores_decode_job_upload(prores_decode_job *job, const prores_buf *in, int n, void *stream) {
     if ((size_t)n != job->plan.frames.size()) return fail(make_status(PRORES_CONFIG, "a job's batch size is fixed"));
     cudaSetDevice(job->ctx->impl.device);
+    job->ctx->impl.refresh(*job->ws);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
     size_t pos = 0;
     for (int i = 0; i < n; i++) {
@@ -888,6 +1006,7 @@ int prores_decode_job_launch(prores_decode_job *job, void *stream, int use_graph
 
 int prores_decode_job_fetch(prores_decode_job *job, void *stream, prores_frame *out, int *status) {
     cudaSetDevice(job->ctx->impl.device);
+    job->ctx->impl.refresh(*job->ws);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : job->ws->stream;
     Status first;
     Status st = fetch_decode(*job->ws, job->plan, s, out, status, &first);
@@ -908,7 +1027,12 @@ int prores_job_kernel_times(const void *job, int is_encode, const char **names, 
     const KernelTimes &kt = is_encode ? static_cast<const prores_encode_job *>(job)->kt
                                       : static_cast<const prores_decode_job *>(job)->kt;
     if (!kt.enabled || kt.events.size() < 2) return 0;
-    if (cudaEventSynchronize(kt.events.back()) != cudaSuccess) return fail(make_status(PRORES_DEVICE, "event"));
+    const uint32_t limit = is_encode ? static_cast<const prores_encode_job *>(job)->ws->wait_ms
+                                     : static_cast<const prores_decode_job *>(job)->ws->wait_ms;
+    {
+        Status st = cuda_status(wait_event(kt.events.back(), limit), "kernel times");
+        if (st) return fail(st);
+    }
     int n = 0;
     for (size_t i = 1; i < kt.events.size() && n < cap; i++, n++) {
         float t = 0;
@@ -922,11 +1046,13 @@ int prores_job_kernel_times(const void *job, int is_encode, const char **names, 
 void prores_decode_job_destroy(prores_decode_job *job) {
     if (!job) return;
     cudaSetDevice(job->ctx->impl.device);
-    if (job->graph) cudaGraphExecDestroy(job->graph);
     for (auto e : job->kt.events) cudaEventDestroy(e);
     if (job->ws) {
-        cudaStreamSynchronize(job->ws->stream);
-        job->ctx->impl.release(std::move(job->ws));
+        // Its work may still run (a fetch that timed out): the workspace and
+        // graph are then kept until it is done.
+        job->ctx->impl.release_or_retire(std::move(job->ws), job->graph);
+    } else if (job->graph) {
+        cudaGraphExecDestroy(job->graph);
     }
     delete job;
 }

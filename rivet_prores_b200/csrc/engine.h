@@ -25,6 +25,7 @@ struct DeviceBuf {
     void *p = nullptr;
     size_t cap = 0;
     cudaStream_t stream = nullptr;
+    uint32_t wait_ms = 0;  // bound on the wait for a growth (0: none)
     cudaError_t reserve(size_t bytes);
     template <class T>
     T *as() const {
@@ -50,6 +51,7 @@ struct Stager {
     static constexpr size_t kChunk = 8u << 20;
     PinnedBuf buf;
     cudaEvent_t ev[kSlots] = {};
+    uint32_t wait_ms = 0;  // bound on each wait for a chunk (0: none)
     struct Pending {
         uint8_t *dst = nullptr;  // host destination of a chunk read back
         size_t len = 0;
@@ -60,6 +62,9 @@ struct Stager {
     cudaError_t d2h(void *dst, const void *src, size_t len, cudaStream_t s);
     // Waits for the chunks still read back and copies them out.
     cudaError_t finish();
+    // Forgets chunks read back for a call that gave up: their host
+    // destinations belong to that call's caller.
+    void forget();
 
   private:
     cudaError_t slot(int &i);  // the next slot, free for the host
@@ -67,9 +72,22 @@ struct Stager {
 
 bool is_page_locked(const void *p);
 
+// The library's default bound on a host wait for the device, in ms.
+constexpr uint32_t kDefaultWaitMs = 60000;
+
+// Waits until event `e` has completed, polling, for at most `limit_ms` (0:
+// no bound). cudaErrorNotReady when the bound ran out first; the event's
+// work is then still in flight.
+cudaError_t wait_event(cudaEvent_t e, uint32_t limit_ms);
+// Waits for everything enqueued on `s` so far the same way. PRORES_TIMEOUT
+// when the bound runs out (the work is left running), PRORES_DEVICE on a
+// CUDA failure.
+Status wait_stream(cudaStream_t s, uint32_t limit_ms, const char *what);
+
 // Per-call device state: a stream and the buffers a batch needs.
 struct Workspace {
     int device = 0;
+    uint32_t wait_ms = kDefaultWaitMs;  // the context's bound when the workspace was taken
     cudaStream_t stream = nullptr;
     DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter;
     // encode
@@ -111,11 +129,25 @@ struct Context {
     // moment; a CUDA graph keeps those it was captured with.
     Tuning tuning;
     EntropyShape entropy{8, 0};
+    // Bound on every host wait for the device (prores_set_timeout).
+    uint32_t wait_ms = kDefaultWaitMs;
     Tuning current_tuning();
     EntropyShape current_entropy();
     std::vector<std::unique_ptr<Workspace>> free_ws;
+    // Workspaces whose stream still had work when a wait ran out or their
+    // call gave up: reused once that work is done, never before.
+    struct Retired {
+        std::unique_ptr<Workspace> ws;
+        cudaGraphExec_t graph = nullptr;  // destroyed with it
+    };
+    std::vector<Retired> retired;
     std::unique_ptr<Workspace> acquire();
     void release(std::unique_ptr<Workspace> ws);
+    // Returns `ws` to the pool if its stream is idle, else keeps it (and
+    // `graph`) aside until it is.
+    void release_or_retire(std::unique_ptr<Workspace> ws, cudaGraphExec_t graph = nullptr);
+    // Gives a job's workspace the context's current wait bound.
+    void refresh(Workspace &ws);
     ~Context();
 };
 
@@ -182,6 +214,9 @@ Status fetch_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_t 
                     int *status, Status *first_err);
 
 void set_last_error(const Status &s);
+// The same with messages already displayed (taken from another thread's).
+void set_last_error_text(const std::string &text);
+void set_batch_error_texts(const std::vector<std::string> &texts);
 // prores_probe's work: the frame header, checked, as sizes and metadata.
 Status probe_frame(const uint8_t *data, size_t len, uint32_t out_bit_depth, prores_frame *info);
 // Per-frame messages of the last batch call on this thread.

@@ -197,7 +197,10 @@ class Server:
         # the callers keep them.
         self.done: List[tuple] = []
         self.batches: List[int] = []
+        # (kind, frames, start, end) of every batch call into the library.
+        self.calls: List[tuple] = []
         self.peak_in_use = 0
+        self.peak_queue = 0
         self.threads = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
         for t in self.threads:
             t.start()
@@ -223,6 +226,7 @@ class Server:
             if self.closed:
                 raise RuntimeError("server closed")
             self.queue.append(r)
+            self.peak_queue = max(self.peak_queue, len(self.queue))
             self.cv.notify_all()
         return r.future
 
@@ -261,6 +265,7 @@ class Server:
                         if batch:
                             break
                     self.cv.wait(0.05)
+            t_call = time.perf_counter()
             try:
                 results = self.backend.decode(batch) if batch[0].kind == "decode" else self.backend.encode(batch)
                 exc = None
@@ -270,6 +275,7 @@ class Server:
             with self.cv:
                 self.in_use -= sum(r.cost for r in batch)
                 self.batches.append(len(batch))
+                self.calls.append((batch[0].kind, len(batch), t_call, now))
                 for r in batch:
                     r.t_done = now
                     self.done.append((r.t_submit, now))
@@ -290,23 +296,51 @@ class Server:
 
     # -------------------------------------------------------------- metrics
 
-    def stats(self) -> dict:
+    def stats(self, window: float = 0.0) -> dict:
+        """Latency percentiles, throughput and batching; with `window`
+        seconds, the same per window of submission time (whether the queue
+        is stationary), and where a request's time went: waiting for a
+        worker, or in the batch call that served it."""
         with self.cv:
-            lat = sorted((d - a) * 1000.0 for a, d in self.done)
+            done = list(self.done)
             batches = list(self.batches)
-            first = min((a for a, _ in self.done), default=0.0)
-            last = max((d for _, d in self.done), default=0.0)
-        if not lat:
+            calls = list(self.calls)
+        if not done:
             return {"requests": 0}
-        pct = lambda p: lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
-        return {"requests": len(lat), "p50_ms": round(pct(50), 3), "p99_ms": round(pct(99), 3),
-                "max_ms": round(lat[-1], 3), "frames_per_s": round(len(lat) / max(last - first, 1e-9), 2),
-                "batches": len(batches), "mean_batch": round(float(np.mean(batches)), 2),
-                "peak_device_bytes_admitted": self.peak_in_use}
+        lat = sorted((d - a) * 1000.0 for a, d in done)
+        first = min(a for a, _ in done)
+        last = max(d for _, d in done)
+        out = {"requests": len(lat), "p50_ms": round(_pct(lat, 50), 3), "p99_ms": round(_pct(lat, 99), 3),
+               "max_ms": round(lat[-1], 3), "frames_per_s": round(len(lat) / max(last - first, 1e-9), 2),
+               "batches": len(batches), "mean_batch": round(float(np.mean(batches)), 2),
+               "peak_device_bytes_admitted": self.peak_in_use, "peak_queue": self.peak_queue}
+        for kind in ("decode", "encode"):
+            mine = [c for c in calls if c[0] == kind]
+            if mine:
+                ms = sorted((e - b) * 1000.0 for _, _, b, e in mine)
+                out[f"{kind}_calls"] = {"count": len(mine), "mean_frames": round(float(np.mean([n for _, n, _, _ in mine])), 2),
+                                        "p50_ms": round(_pct(ms, 50), 3), "p99_ms": round(_pct(ms, 99), 3)}
+        if window > 0:
+            wins = []
+            k = 0
+            while first + k * window < max(a for a, _ in done) + 1e-9:
+                lo, hi = first + k * window, first + (k + 1) * window
+                w = sorted((d - a) * 1000.0 for a, d in done if lo <= a < hi)
+                if w:
+                    wins.append({"t0_s": round(k * window, 1), "requests": len(w), "p50_ms": round(_pct(w, 50), 3),
+                                 "p99_ms": round(_pct(w, 99), 3),
+                                 "completed_per_s": round(sum(1 for _, d in done if lo <= d < hi) / window, 1)})
+                k += 1
+            out["windows"] = wins
+        return out
+
+
+def _pct(sorted_ms, p):
+    return sorted_ms[min(len(sorted_ms) - 1, int(round(p / 100.0 * (len(sorted_ms) - 1))))]
 
 
 def poisson_run(server: Server, make_request: Callable[[int], tuple], rate: float, seconds: float,
-                seed: int = 0) -> dict:
+                seed: int = 0, window: float = 0.0) -> dict:
     """Submits requests at Poisson times (mean `rate` per second) for
     `seconds`; make_request(i) gives ("decode", data) or ("encode", frame,
     config). Each result is dropped as it arrives, as a client that consumes
@@ -345,7 +379,7 @@ def poisson_run(server: Server, make_request: Callable[[int], tuple], rate: floa
     with lock:
         while state["finished"] < state["submitted"]:
             lock.wait(1.0)
-    s = server.stats()
+    s = server.stats(window)
     s["offered_rate"] = rate
     s["seconds"] = seconds
     s["errors"] = state["errors"]

@@ -13,7 +13,9 @@ def macroblocks(width: int, height: int) -> int:
 
 def shard_by_macroblocks(sizes: Sequence[Tuple[int, int]], world: int) -> List[List[int]]:
     """Frame indices for each rank: the largest frames first, each to the rank
-    with the fewest macroblocks so far (ties to the lower rank)."""
+    with the fewest macroblocks so far (ties to the lower rank). The same
+    split as the library's prores_shard_frames, which its multi-device batch
+    calls use."""
     order = sorted(range(len(sizes)), key=lambda i: (-macroblocks(*sizes[i]), i))
     load = [0] * world
     shards: List[List[int]] = [[] for _ in range(world)]

@@ -14,11 +14,22 @@ noise, clamped).
 
 from __future__ import annotations
 
-from typing import List, Optional
+import os
+from concurrent.futures import ThreadPoolExecutor
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 
-from . import ChromaFormat, Config, Frame, Interlace, Profile
+from . import AlphaType, ChromaFormat, Config, Frame, Interlace, Profile
+
+
+def generate(makers: Sequence[Callable[[], object]]) -> list:
+    """Runs the picture makers on host threads (numpy's array work releases
+    the GIL), in order."""
+    if len(makers) <= 1:
+        return [m() for m in makers]
+    with ThreadPoolExecutor(max_workers=min(len(makers), os.cpu_count() or 4)) as ex:
+        return list(ex.map(lambda m: m(), makers))
 
 
 def _plane(h: int, w: int, rng: np.random.Generator, hi: float) -> np.ndarray:
@@ -80,8 +91,61 @@ def uhd_422_hq(n: int, config: int = 1, unique: Optional[int] = None) -> List[Fr
     """n 3840x2160 4:2:2 10-bit frames (the 422 HQ headline workload); with
     `unique`, that many distinct pictures repeated."""
     u = n if unique is None else max(1, min(unique, n))
-    base = [picture(3840, 2160, ChromaFormat.Yuv422, 10, 1000 * config + i) for i in range(u)]
+    base = generate([lambda i=i: picture(3840, 2160, ChromaFormat.Yuv422, 10, 1000 * config + i)
+                     for i in range(u)])
     return [base[i % u] for i in range(n)]
+
+
+def uhd_422_hq_at(indices: Sequence[int], config: int = 1) -> List[Frame]:
+    """Frames `indices` of the headline batch (3840x2160 4:2:2 10-bit, the
+    seed of frame i is 1000 * config + i): one rank's share of a batch
+    split over ranks."""
+    return generate([lambda i=i: picture(3840, 2160, ChromaFormat.Yuv422, 10, 1000 * config + i)
+                     for i in indices])
+
+
+def hd_422_hq(n: int = 64, config: int = 1):
+    """Batched 1080p decode: n 1920x1080 4:2:2 10-bit frames with per-frame
+    seeds, to be coded as 422 HQ at the profile's target. [(frame, config)]"""
+    frames = generate([lambda i=i: picture(1920, 1080, ChromaFormat.Yuv422, 10, 1000 * config + i)
+                       for i in range(n)])
+    return [(f, Config(Profile.Hq)) for f in frames]
+
+
+def uhd_4444xq_alpha(n: int = 16, config: int = 2):
+    """n 3840x2160 4:4:4 12-bit frames with a 16-bit alpha plane, interlaced
+    top field first, each with its own loaded luma and chroma matrices
+    (entries U(4, 63)), coded as 4444 XQ. [(frame, config)]"""
+    frames = generate([lambda i=i: picture(3840, 2160, ChromaFormat.Yuv444, 12, 1000 * config + i, alpha=True,
+                                           interlace=Interlace.TopFieldFirst) for i in range(n)])
+    return [(f, Config(Profile.P4444Xq, alpha=AlphaType.Bits16, luma_matrix=matrix(1000 * config + i),
+                       chroma_matrix=matrix(1000 * config + 100 + i))) for i, f in enumerate(frames)]
+
+
+MIXED_KINDS = [
+    (720, 486, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.BottomFieldFirst, False),
+    (1280, 720, ChromaFormat.Yuv422, 10, Profile.Lt, Interlace.Progressive, False),
+    (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Proxy, Interlace.Progressive, False),
+    (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Standard, Interlace.Progressive, False),
+    (1920, 1080, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.Progressive, False),
+    (3840, 2160, ChromaFormat.Yuv422, 10, Profile.Hq, Interlace.Progressive, False),
+    (4096, 2160, ChromaFormat.Yuv444, 16, Profile.P4444, Interlace.Progressive, True),
+]
+
+
+def mixed_batch(n: int = 96, config: int = 3):
+    """The heterogeneous batch: n frames cycling through the mix's kinds
+    (720x486 interlaced 422 HQ, 1280x720 LT, 1920x1080 Proxy / 422 / HQ,
+    3840x2160 HQ, 4096x2160 4444 from 16-bit input with a 16-bit alpha
+    plane), per-frame seeds, each with a slice width drawn from {1, 2, 4, 8}
+    macroblocks. [(frame, config)]"""
+    rng = np.random.Generator(np.random.PCG64([1000 * config, 98]))
+    kinds = [MIXED_KINDS[i % len(MIXED_KINDS)] for i in range(n)]
+    log2s = [int(v) for v in rng.integers(0, 4, n)]
+    frames = generate([lambda i=i, k=k: picture(k[0], k[1], k[2], k[3], 1000 * config + i, alpha=k[6],
+                                                interlace=k[5]) for i, k in enumerate(kinds)])
+    return [(f, Config(k[4], log2_slice_mbs=l, alpha=AlphaType.Bits16 if k[6] else AlphaType.None_))
+            for f, k, l in zip(frames, kinds, log2s)]
 
 
 def hq_config() -> Config:

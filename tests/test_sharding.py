@@ -60,3 +60,26 @@ def test_two_ranks_split_the_frames_and_agree_on_the_slowest():
     (_, a, ga), (_, b, gb) = res
     assert sorted(a + b) == list(range(5)) and not set(a) & set(b)
     assert ga == gb
+
+
+def test_the_split_is_the_librarys():
+    """shard_by_macroblocks (ranks under torchrun) and prores_shard_frames
+    (the library's multi-device batch calls) split alike."""
+    import ctypes
+
+    import numpy as np
+
+    from rivet_prores_b200 import _abi
+
+    rng = np.random.Generator(np.random.PCG64(5))
+    kinds = [(3840, 2160), (4096, 2160), (1920, 1080), (1280, 720), (720, 486), (16, 16), (33, 17)]
+    for trial in range(50):
+        n = int(rng.integers(0, 40))
+        sizes = [kinds[int(k)] for k in rng.integers(0, len(kinds), n)]
+        world = int(rng.integers(1, 9))
+        w = (ctypes.c_uint32 * max(n, 1))(*[s[0] for s in sizes])
+        h = (ctypes.c_uint32 * max(n, 1))(*[s[1] for s in sizes])
+        part = (ctypes.c_int * max(n, 1))()
+        assert _abi.lib().prores_shard_frames(w, h, n, world, part) == _abi.OK
+        lib_split = [[i for i in range(n) if part[i] == r] for r in range(world)]
+        assert lib_split == shard_by_macroblocks(sizes, world), (trial, sizes, world)
