@@ -255,8 +255,12 @@ int prores_encode_device(prores_ctx *ctx, const prores_config *cfg, const prores
 
 /* ---- decode without device allocation --------------------------------- */
 
-/* Size of the fixed device array prores_decode_noalloc keeps its scratch in:
- * enough for any frame up to 1920x1080, 4:2:2 or 4:4:4. */
+/* Size of the fixed device array prores_decode_noalloc keeps its scratch in.
+ * A frame fits when 4 bytes per coefficient position (512 positions per
+ * 4:2:2 macroblock, 768 per 4:4:4 one), its frame_size bytes and 64 bytes
+ * per slice, plus 21 KiB, come to no more than this: every 1920x1080 frame
+ * whose packet is under about 40 MB (4:4:4) or 50 MB (4:2:2); UHD frames
+ * do not fit. */
 #define PRORES_NOALLOC_SCRATCH_BYTES (64u << 20)
 
 /* Decodes one frame, like prores_decode, without allocating any device
@@ -270,7 +274,7 @@ int prores_encode_device(prores_ctx *ctx, const prores_config *cfg, const prores
  * for a frame without alpha; prores_probe gives both sizes). The decoder's
  * scratch lives in one static device array of PRORES_NOALLOC_SCRATCH_BYTES
  * that every GPU which loads it holds until the process exits; a frame that
- * needs more (larger than 1920x1080) is refused with PRORES_CONFIG. No
+ * needs more (see PRORES_NOALLOC_SCRATCH_BYTES) is refused with PRORES_CONFIG. No
  * context is needed: the first call on a device sets that device up (the
  * array's address, the kernels' settings, the decoder's tables), so make that
  * first call before any stream capture. Every call shares the one array; the
@@ -335,6 +339,16 @@ typedef struct prores_tuning {
     /* Batches a caller keeps in flight when it streams host buffers through
      * jobs (1-64): stored for the caller, read by no kernel. */
     int32_t staging_depth;
+    /* Decoder: 1 runs the per-slice decode as one kernel (entropy decoding
+     * into shared memory, then the IDCT and stores, per group of slices);
+     * 0 as two (entropy decoding into lists in device memory, then the
+     * IDCT). decode_slot_positions (512-65536): coefficient positions one
+     * CTA of the fused kernel holds, which sets how many slices it takes
+     * at once; decode_slot_bytes (1 or 2): the bytes each takes there (a
+     * value the type cannot hold goes through device memory). */
+    int32_t decode_fused;
+    int32_t decode_slot_positions;
+    int32_t decode_slot_bytes;
 } prores_tuning;
 
 void prores_tuning_default(prores_tuning *t);

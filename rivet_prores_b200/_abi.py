@@ -94,6 +94,9 @@ class Tuning_(ctypes.Structure):
         ("entropy_blocks_per_sm", ctypes.c_int32),
         ("entropy_components_per_lane", ctypes.c_int32),
         ("staging_depth", ctypes.c_int32),
+        ("decode_fused", ctypes.c_int32),
+        ("decode_slot_positions", ctypes.c_int32),
+        ("decode_slot_bytes", ctypes.c_int32),
     ]
 
 

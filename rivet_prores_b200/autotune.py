@@ -6,10 +6,13 @@ The shapes are the fields of `Tuning` (prores_tuning in the C ABI):
   which rate-control costing runs a lane per slice component rather than a
   warp per component. Lanes need many components to fill the GPU; warps
   finish a small batch sooner.
+* `decode_fused`, `decode_slot_positions`: whether the per-slice decode
+  runs as one kernel, and how many coefficient positions (so how many
+  slices) one of its CTAs holds in shared memory at once.
 * `entropy_warps_per_block`, `entropy_blocks_per_sm`,
-  `entropy_components_per_lane`: the persistent entropy decoder's warps per
-  CTA, resident CTAs per SM and slice components per lane per grab of the
-  shared work counter.
+  `entropy_components_per_lane`: for the two-kernel decode, the persistent
+  entropy decoder's warps per CTA, resident CTAs per SM and slice
+  components per lane per grab of the shared work counter.
 * `staging_depth`: the parts a batch of host frames is split into when it is
   streamed through resident jobs (`stream.RoundTripPipeline`): copies of one
   part overlap the kernels of another.
@@ -197,23 +200,34 @@ def tune(device: int = 0, quick: bool = False, store: bool = True, frames: Optio
     enc.close()
     dec = DecodeJob(packets, device=device)
     shapes = {}
-    warps = [4, 8, 16]
-    blocks = [0, 2] if quick else [0, 1, 2, 3]
-    per_lane = [1, 2] if quick else [1, 2, 4]
+    # The fused decoder by slice group size ...
+    for nbytes in (1, 2):
+        for pos in ([8192, 16384, 32768] if quick else [4096, 8192, 12288, 16384, 24576, 32768, 49152]):
+            ctx.set_tuning(type(tuning)(**{**asdict(tuning), "decode_fused": 1, "decode_slot_positions": pos,
+                                           "decode_slot_bytes": nbytes}))
+            shapes[(1, pos, nbytes, 0, 0, 0)] = _time(lambda: dec.launch(stream), stream, reps)
+    # ... against the two-kernel form's shapes.
+    warps = [8] if quick else [4, 8, 16]
+    blocks = [0] if quick else [0, 1, 2, 3]
+    per_lane = [1] if quick else [1, 2, 4]
     for w in warps:
         for b in blocks:
             for k in per_lane:
-                cand = type(tuning)(**{**asdict(tuning), "entropy_warps_per_block": w, "entropy_blocks_per_sm": b,
-                                       "entropy_components_per_lane": k})
+                cand = type(tuning)(**{**asdict(tuning), "decode_fused": 0, "entropy_warps_per_block": w,
+                                       "entropy_blocks_per_sm": b, "entropy_components_per_lane": k})
                 ctx.set_tuning(cand)
-                shapes[(w, b, k)] = _time(lambda: dec.launch(stream), stream, reps)
+                shapes[(0, tuning.decode_slot_positions, tuning.decode_slot_bytes, w, b, k)] = _time(
+                    lambda: dec.launch(stream), stream, reps)
     dec.close()
-    w, b, k = best(shapes)
-    tuning = type(tuning)(**{**asdict(tuning), "entropy_warps_per_block": w, "entropy_blocks_per_sm": b,
-                             "entropy_components_per_lane": k})
-    evidence["entropy"] = [{"warps_per_block": a, "blocks_per_sm": c, "components_per_lane": d, "ms": round(v, 4)}
-                           for (a, c, d), v in shapes.items()]
-    say(f"entropy: {w} warps/block, {b} blocks/SM, {k} per lane ({shapes[(w, b, k)]:.3f} ms)")
+    fused, pos, nbytes, w, b, k = best(shapes)
+    chosen = {"decode_fused": fused, "decode_slot_positions": pos, "decode_slot_bytes": nbytes}
+    if not fused:
+        chosen.update(entropy_warps_per_block=w, entropy_blocks_per_sm=b, entropy_components_per_lane=k)
+    tuning = type(tuning)(**{**asdict(tuning), **chosen})
+    evidence["decode"] = [{"fused": a, "slot_positions": p, "slot_bytes": q, "warps_per_block": c,
+                           "blocks_per_sm": d, "components_per_lane": e, "ms": round(v, 4)}
+                          for (a, p, q, c, d, e), v in shapes.items()]
+    say(f"decode: {chosen} ({shapes[(fused, pos, nbytes, w, b, k)]:.3f} ms)")
 
     # Staging depth of the host round trip.
     ctx.set_tuning(tuning)

@@ -21,7 +21,7 @@ LIB = os.path.join(OUT_DIR, "libprores_b200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-Wall"]
 
 

@@ -152,4 +152,16 @@ inline void build_decode_table(Books books, int n_books, uint16_t *out) {
     }
 }
 
+// One row per distinct codebook, for decoders that map a context to its
+// codebook: Table 10's run codebooks for previousRun 0-1, 2-3, 4, 5-8, 9-14,
+// 15+ and Table 11's level codebooks for previousLevelSymbol 0, 1, 2, 3,
+// 4-7, 8+ (the first context of each range stands for it).
+static constexpr uint32_t kBookTableWords = 6 * kDecodeEntries;
+inline void build_book_tables(uint16_t *run, uint16_t *level) {
+    static const uint32_t run_ctx[6] = {0, 2, 4, 5, 9, 15};
+    static const uint32_t level_ctx[6] = {0, 1, 2, 3, 4, 8};
+    build_decode_table([&](uint32_t i) { return run_book(run_ctx[i]); }, 6, run);
+    build_decode_table([&](uint32_t i) { return level_book(level_ctx[i]); }, 6, level);
+}
+
 }  // namespace prores

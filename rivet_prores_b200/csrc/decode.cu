@@ -42,11 +42,13 @@ __device__ __forceinline__ uint32_t be16(const uint8_t *p) { return ((uint32_t)p
 
 // MSB-first reader over [start, end) bits of the bitstream buffer: a pair of
 // aligned 64-bit words funnel-shifted to the position; bits past `end` read
-// as zero (the crate's BitReader::peek64, src/bits.rs:30-40). The buffer has
-// at least 16 bytes of padding, so the second word never leaves it.
+// as zero (the crate's BitReader::peek64, src/bits.rs:30-40). The word after
+// the pair is fetched one word ahead, so moving on to the next word never
+// waits for memory. The buffer has at least 24 bytes of padding after the
+// last data word, so the words read never leave it.
 struct Bits {
     const uint64_t *w;
-    uint64_t pos, end, idx, w0, w1;
+    uint64_t pos, end, idx, w0, w1, w2;
 
     __device__ __forceinline__ uint64_t ld(uint64_t i) const { return bswap64(__ldg(w + i)); }
     __device__ __forceinline__ void init(const uint8_t *base, uint64_t byte_off, uint64_t len) {
@@ -56,6 +58,7 @@ struct Bits {
         idx = pos >> 6;
         w0 = ld(idx);
         w1 = ld(idx + 1);
+        w2 = ld(idx + 2);
     }
     __device__ __forceinline__ uint64_t remaining() const { return end - pos; }
     __device__ __forceinline__ uint64_t peek() {
@@ -63,10 +66,12 @@ struct Bits {
         if (i != idx) {
             if (i == idx + 1) {
                 w0 = w1;
-                w1 = ld(i + 1);
+                w1 = w2;
+                w2 = ld(i + 2);
             } else {
                 w0 = ld(i);
                 w1 = ld(i + 1);
+                w2 = ld(i + 2);
             }
             idx = i;
         }
@@ -142,14 +147,38 @@ constexpr int32_t kListMin = -(1 << 20) + 2048;
 
 struct CoefList {
     uint32_t *w;
-    uint32_t cap, big;
-    __device__ __forceinline__ void put(uint32_t &count, uint32_t n, int32_t v) {
+    uint32_t cap, big, count;
+    __device__ __forceinline__ void put(uint32_t n, int32_t v) {
         if (v >= kListMin && v < (1 << 20)) {
             w[count++] = (n << 21) | ((uint32_t)v & 0x1FFFFFu);
         } else {
             w[2u * cap - 1u - big] = (uint32_t)v;
             w[count++] = (n << 21) | ((uint32_t)(-(1 << 20) + (int32_t)big) & 0x1FFFFFu);
             big++;
+        }
+    }
+};
+
+// A component's coefficients as one small integer (int8_t or int16_t) per
+// scanned position in shared memory (zeroed beforehand: only the coded ones
+// are written). A value the type cannot hold, other than its most negative
+// one, is marked with that one (wide_mark<T>) and kept at the same position
+// of a 32-bit array in global memory, which is otherwise never touched.
+template <class T>
+__device__ __forceinline__ constexpr int32_t wide_mark() {
+    return sizeof(T) == 1 ? -128 : -32768;
+}
+
+template <class T>
+struct SlotOut {
+    T *slot;
+    int32_t *wide;
+    __device__ __forceinline__ void put(uint32_t n, int32_t v) {
+        if (v > wide_mark<T>() && v <= -(wide_mark<T>() + 1)) {
+            slot[n] = (T)v;
+        } else {
+            slot[n] = (T)wide_mark<T>();
+            wide[n] = v;
         }
     }
 };
@@ -161,17 +190,35 @@ __device__ __forceinline__ void list_entry(const uint32_t *w, uint32_t cap, uint
     if (v < kListMin) v = (int32_t)__ldg(w + 2u * cap - 1u - (uint32_t)(v + (1 << 20)));
 }
 
+// Prefix-table rows by context: the rows of `run_tab` and `level_tab` are
+// either one per context (16 run, 9 level contexts) or one per distinct
+// codebook (Tables 10 and 11 have 6 each), as `Rows` says.
+struct ContextRows {
+    __device__ __forceinline__ static uint32_t run(uint32_t ctx) { return ctx < 15u ? ctx : 15u; }
+    __device__ __forceinline__ static uint32_t level(uint32_t ctx) { return ctx < 8u ? ctx : 8u; }
+};
+struct BookRows {
+    // Table 10: previousRun 0-1, 2-3, 4, 5-8, 9-14, 15+ share a codebook;
+    // Table 11: previousLevelSymbol 0, 1, 2, 3, 4-7, 8+.
+    __device__ __forceinline__ static uint32_t run(uint32_t ctx) {
+        return (uint32_t)(0x5444444333321100ull >> (4u * (ctx < 15u ? ctx : 15u))) & 15u;
+    }
+    __device__ __forceinline__ static uint32_t level(uint32_t ctx) {
+        return (uint32_t)(0x544443210ull >> (4u * (ctx < 8u ? ctx : 8u))) & 15u;
+    }
+};
+
 // scanned_coefficients() of one component (src/decode.rs:484-540): every
-// coefficient the codes give, as (scanned index, value) entries in index
-// order; `count` gets how many (also when decoding fails part-way).
-__device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32_t &count, const uint16_t *run_tab,
+// coefficient the codes give, in scanned-index order, handed to `out.put`
+// (position, value); the positions not handed over are zero.
+template <class Rows = ContextRows, class Out>
+__device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
-    count = 0;
     uint32_t sym;
     int err = read_sym(b, nullptr, kFirstDcBook, sym);
     if (err) return err;
     int32_t prev_dc = symbol_to_signed(sym);
-    out.put(count, 0, prev_dc);
+    out.put(0, prev_dc);
     int32_t prev_diff = 3;
     for (uint32_t i = 1; i < n_blocks; i++) {
         if ((err = read_sym(b, nullptr, dc_book(prev_diff), sym))) return err;
@@ -180,7 +227,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32
         int64_t s = (int64_t)prev_dc + diff;
         if (s > INT32_MAX || s < INT32_MIN) return DE_DC_OVERFLOW;
         prev_dc = (int32_t)s;
-        out.put(count, i, prev_dc);
+        out.put(i, prev_dc);
         prev_diff = diff;
     }
     const uint32_t total = n_blocks * 64;
@@ -191,12 +238,11 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32
         if (rem >= 64) {
             // Run, level and sign from one window when both codewords are
             // in the prefix tables (all 64 window bits are data here).
-            uint32_t e1 = run_tab[(prev_run < 15u ? prev_run : 15u) * kDecodeEntries + (w >> (64 - kDecodeBits))];
+            uint32_t e1 = run_tab[Rows::run(prev_run) * kDecodeEntries + (w >> (64 - kDecodeBits))];
             if (e1) {
                 uint32_t l1 = e1 & 31;
                 uint64_t w2 = w << l1;
-                uint32_t e2 =
-                    level_tab[(prev_level < 8u ? prev_level : 8u) * kDecodeEntries + (w2 >> (64 - kDecodeBits))];
+                uint32_t e2 = level_tab[Rows::level(prev_level) * kDecodeEntries + (w2 >> (64 - kDecodeBits))];
                 if (e2) {
                     uint32_t l2 = e2 & 31;
                     uint32_t run = e1 >> 5, lvl = e2 >> 5;
@@ -205,7 +251,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32
                     int32_t level = (int32_t)lvl + 1;
                     bool neg = (w2 << l2) >> 63;
                     b.pos += l1 + l2 + 1;
-                    out.put(count, n, neg ? -level : level);
+                    out.put(n, neg ? -level : level);
                     n += 1;
                     prev_run = run;
                     prev_level = lvl;
@@ -216,21 +262,18 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, CoefList out, uint32
             break;  // endOfData()
         }
         uint32_t run, lvl;
-        if ((err = read_sym(b, run_tab + (prev_run < 15u ? prev_run : 15u) * kDecodeEntries, run_book(prev_run),
-                            run)))
-            return err;
+        if ((err = read_sym(b, run_tab + Rows::run(prev_run) * kDecodeEntries, run_book(prev_run), run))) return err;
         prev_run = run;
         n += run;
         if (n >= total) return DE_RUN_PAST_END;
-        if ((err = read_sym(b, level_tab + (prev_level < 8u ? prev_level : 8u) * kDecodeEntries,
-                            level_book(prev_level), lvl)))
+        if ((err = read_sym(b, level_tab + Rows::level(prev_level) * kDecodeEntries, level_book(prev_level), lvl)))
             return err;
         prev_level = lvl;
         if (b.remaining() < 1) return DE_PAST_END;
         bool neg = b.peek() >> 63;
         b.pos += 1;
         int32_t level = (int32_t)lvl + 1;
-        out.put(count, n, neg ? -level : level);
+        out.put(n, neg ? -level : level);
         n += 1;
     }
     return DE_OK;
@@ -300,6 +343,44 @@ __device__ int decode_alpha(Bits &b, const FrameDesc &fd, const PicDesc &pd, con
     return DE_OK;
 }
 
+// The slice header (src/decode.rs:301-338) and where component `comp` (0
+// Y', 1 Cb, 2 Cr, 3 alpha) lies in the slice. A header failure comes back
+// (the Y' item reports it; the other components then report nothing).
+__device__ int2 component_range(const uint8_t *sb, uint32_t size, bool has_alpha, uint32_t comp, uint32_t &start,
+                                uint32_t &len) {
+    const uint32_t min_header = has_alpha ? 8u : 6u;
+    uint32_t hs = 0, ys = 0, cbs = 0, crs = 0;
+    if (size < min_header) return make_int2(DE_SLICE_SHORT, 0);
+    hs = sb[0] >> 3;
+    const uint32_t qi = sb[1];
+    if (hs < min_header || hs > size) return make_int2(DE_SLICE_HDR_SIZE, (int)hs);
+    if (qi < 1 || qi > 224) return make_int2(DE_QINDEX, (int)qi);
+    ys = be16(sb + 2);
+    cbs = be16(sb + 4);
+    const uint32_t body = size - hs;
+    if (has_alpha) {
+        crs = be16(sb + 6);
+    } else {
+        if (ys + cbs > body) return make_int2(DE_COMP_SIZES, 0);
+        crs = body - ys - cbs;
+    }
+    if (ys + cbs + crs > body) return make_int2(DE_COMP_SIZES, 0);
+    start = hs;
+    if (comp == 0) {
+        len = ys;
+    } else if (comp == 1) {
+        start += ys;
+        len = cbs;
+    } else if (comp == 2) {
+        start += ys + cbs;
+        len = crs;
+    } else {
+        start += ys + cbs + crs;
+        len = size - start;
+    }
+    return make_int2(DE_OK, 0);
+}
+
 // One work item: component `comp` (0 Y', 1 Cb, 2 Cr, 3 alpha) of slice `s`.
 __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, const uint16_t *run_tab,
                             const uint16_t *level_tab) {
@@ -316,51 +397,11 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
         *slot = make_int2(DE_OK, 0);
         return;
     }
-    // The slice header (src/decode.rs:301-338); the Y' item reports it.
-    const uint8_t *sb = d.bits + sd.off;
-    const uint32_t size = sd.size;
-    const uint32_t min_header = has_alpha ? 8u : 6u;
-    int2 hdr_err = make_int2(DE_OK, 0);
-    uint32_t hs = 0, ys = 0, cbs = 0, crs = 0;
-    if (size < min_header) {
-        hdr_err = make_int2(DE_SLICE_SHORT, 0);
-    } else {
-        hs = sb[0] >> 3;
-        uint32_t qi = sb[1];
-        if (hs < min_header || hs > size) {
-            hdr_err = make_int2(DE_SLICE_HDR_SIZE, (int)hs);
-        } else if (qi < 1 || qi > 224) {
-            hdr_err = make_int2(DE_QINDEX, (int)qi);
-        } else {
-            ys = be16(sb + 2);
-            cbs = be16(sb + 4);
-            uint32_t body = size - hs;
-            if (has_alpha) {
-                crs = be16(sb + 6);
-            } else if (ys + cbs > body) {
-                hdr_err = make_int2(DE_COMP_SIZES, 0);
-            } else {
-                crs = body - ys - cbs;
-            }
-            if (hdr_err.x == DE_OK && ys + cbs + crs > body) hdr_err = make_int2(DE_COMP_SIZES, 0);
-        }
-    }
+    uint32_t start = 0, len = 0;
+    const int2 hdr_err = component_range(d.bits + sd.off, sd.size, has_alpha, comp, start, len);
     if (hdr_err.x != DE_OK) {
         *slot = comp == 0 ? hdr_err : make_int2(DE_OK, 0);
         return;
-    }
-    uint32_t start = hs, len;
-    if (comp == 0) {
-        len = ys;
-    } else if (comp == 1) {
-        start += ys;
-        len = cbs;
-    } else if (comp == 2) {
-        start += ys + cbs;
-        len = crs;
-    } else {
-        start += ys + cbs + crs;
-        len = size - start;
     }
     Bits b;
     b.init(d.bits, sd.off + start, len);
@@ -371,10 +412,9 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
         const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
         const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
         const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
-        uint32_t count = 0;
-        const CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u};
-        err = decode_component(b, n_blocks, list, count, run_tab, level_tab);
-        d.coef_count[3ull * s + comp] = count;
+        CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u, 0u};
+        err = decode_component(b, n_blocks, list, run_tab, level_tab);
+        d.coef_count[3ull * s + comp] = list.count;
     }
     *slot = make_int2(err, 0);
 }
@@ -718,6 +758,257 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
     }
 }
 
+// ------------------------------------------------------------ fused decode
+//
+// k_decode: the whole per-slice chain in one kernel (src/decode.rs:292-391).
+// A CTA takes a group of consecutive slices of the flat list at a time
+// (grabbed from a work counter) and
+//   1. zeroes the group's coefficient slots in shared memory (one int16 per
+//      scanned position of every component) and sets the slices up: where
+//      their positions and blocks start, their dequantisation factors;
+//   2. decodes every component of the group, one thread each (Y' of every
+//      slice, then Cb, Cr, alpha), straight into the slots; alpha goes to
+//      its plane as it is decoded;
+//   3. transforms every block of the group, one thread each, in registers:
+//      dequantise, the 8x8 IDCT in the crate's single-precision order,
+//      conversion, and 16-byte row stores into the woven planes.
+// No coefficient leaves the chip; the bitstream is read once and the planes
+// written once.
+
+constexpr int kDecodeThreads = 128;
+constexpr uint32_t kMaxGroup = 32;  // slices a CTA decodes at once (4 items each <= 128 threads)
+constexpr uint32_t kBookEntries = 6 * kDecodeEntries;  // one prefix-table row per distinct codebook
+
+// Figures 4 and 5, folded into immediates in the unrolled transform:
+// scan_at<IL>(8 v + u) is the scanned index of row v, column u.
+struct ScanPair {
+    uint8_t v[2][64];
+};
+__device__ constexpr ScanPair scan_pair() {
+    ScanPair s{};
+    for (int i = 0; i < 64; i++) {
+        s.v[0][i] = kProgressiveScan[i];
+        s.v[1][i] = kInterlacedScan[i];
+    }
+    return s;
+}
+template <int IL>
+__device__ __forceinline__ constexpr uint32_t scan_at(int i) {
+    constexpr ScanPair s = scan_pair();
+    return s.v[IL][i];
+}
+
+// A slice of a CTA's group.
+struct GroupSlice {
+    uint32_t pos;         // its first position in the group's slots
+    uint32_t blk;         // its first block in the group's list of blocks
+    uint32_t nb_y, nb_c;  // blocks of Y' and of each chroma component
+    uint32_t live;        // decoded at all (its picture's slices were located)
+};
+
+// q exactly, for |q| < 2^22: q added to the significand of 1.5 2^23.
+__device__ __forceinline__ float small_int_to_float(int32_t q) {
+    return __fadd_rn(__int_as_float(0x4B400000 + q), -12582912.0f);
+}
+
+// floor(v) clamped to [0, max] (max an integer below 2^16), as an integer:
+// clamping before the floor gives the same value as after it for integer
+// bounds, and adding 2^23 rounded down leaves floor(v) in the low bits.
+__device__ __forceinline__ uint32_t floor_clamped(float v, float max) {
+    const float c = fminf(fmaxf(v, 0.0f), max);
+    return __float_as_uint(__fadd_rd(c, 8388608.0f)) & 0xFFFFu;
+}
+
+// One block: dequantise (F = QF scale, src/dsp/scalar.rs:8-12), the IDCT's
+// row pass tmp[v][x] = sum_u F[v][u] T[x][u] and column pass
+// f[y][x] = sum_v T[y][v] tmp[v][x], each sum in the crate's order
+// (src/dct.rs:36-66), then floor(f s + b) clamped, stored row by row. Every
+// term is computed: a zero term adds nothing to a non-zero sum and only
+// flips the sign of a zero one, which the conversion cannot see, so the
+// crate's skipped zero rows and its leading 0 + come out the same.
+template <int IL, class T>
+__device__ __forceinline__ void idct_block(const T *cs, const int32_t *wide, uint32_t nb, uint32_t blk,
+                                           const float *sc, float oscale, float obias, float omax, uint16_t *row0,
+                                           uint64_t row_pitch, uint32_t cols, uint32_t rows) {
+    float t[64];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        float f[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const uint32_t n = scan_at<IL>(8 * v + u) * nb + blk;
+            const int32_t q = cs[n];
+            const float fq = q == wide_mark<T>() ? __int2float_rn(wide[n]) : small_int_to_float(q);
+            f[u] = __fmul_rn(fq, sc[8 * v + u]);
+        }
+#pragma unroll
+        for (int x = 0; x < 8; x++) {
+            float acc = __fmul_rn(f[0], c_idct_basis[8 * x]);
+#pragma unroll
+            for (int u = 1; u < 8; u++) acc = __fadd_rn(acc, __fmul_rn(f[u], c_idct_basis[8 * x + u]));
+            t[8 * v + x] = acc;
+        }
+    }
+#pragma unroll
+    for (int y = 0; y < 8; y++) {
+        uint32_t px[8];
+#pragma unroll
+        for (int x = 0; x < 8; x++) {
+            float acc = __fmul_rn(c_idct_basis[8 * y], t[x]);
+#pragma unroll
+            for (int v = 1; v < 8; v++) acc = __fadd_rn(acc, __fmul_rn(c_idct_basis[8 * y + v], t[8 * v + x]));
+            px[x] = floor_clamped(__fadd_rn(__fmul_rn(acc, oscale), obias), omax);
+        }
+        if ((uint32_t)y >= rows) continue;
+        uint16_t *dst = row0 + (uint64_t)y * row_pitch;
+        if (cols == 8u && (reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+            uint4 w;
+            w.x = __byte_perm(px[0], px[1], 0x5410);
+            w.y = __byte_perm(px[2], px[3], 0x5410);
+            w.z = __byte_perm(px[4], px[5], 0x5410);
+            w.w = __byte_perm(px[6], px[7], 0x5410);
+            __stcs(reinterpret_cast<uint4 *>(dst), w);
+        } else {
+#pragma unroll
+            for (int x = 0; x < 8; x++)
+                if ((uint32_t)x < cols) dst[x] = (uint16_t)px[x];
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kDecodeThreads) k_decode(DecodeLaunch d) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint16_t *run_tab = reinterpret_cast<uint16_t *>(smem);
+    uint16_t *level_tab = run_tab + kBookEntries;
+    GroupSlice *gs = reinterpret_cast<GroupSlice *>(level_tab + kBookEntries);  // kMaxGroup
+    float *scale = reinterpret_cast<float *>(gs + kMaxGroup);                    // [group][luma, chroma][64]
+    T *slots = reinterpret_cast<T *>(scale + 128u * d.group);                   // group_positions
+    __shared__ uint32_t s_group, s_blocks;
+
+    for (uint32_t i = threadIdx.x; i < kBookEntries / 2; i += kDecodeThreads) {
+        reinterpret_cast<uint32_t *>(run_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.run_books)[i];
+        reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_books)[i];
+    }
+    const uint32_t n_groups = (d.n_slices + d.group - 1u) / d.group;
+    int32_t *wide_all = reinterpret_cast<int32_t *>(d.coef);
+    for (;;) {
+        __syncthreads();  // the last group's blocks are all transformed (and the tables are in)
+        if (threadIdx.x == 0) s_group = atomicAdd(d.work_counter, 1u);
+        __syncthreads();
+        const uint32_t g = s_group;
+        if (g >= n_groups) break;
+        const uint32_t first = g * d.group;
+        const uint32_t count = min(d.group, d.n_slices - first);
+
+        // 1. Zeroed slots; the slices' places in the group.
+        for (uint32_t i = threadIdx.x; i < d.group_positions * sizeof(T) / 16u; i += kDecodeThreads)
+            reinterpret_cast<int4 *>(slots)[i] = make_int4(0, 0, 0, 0);
+        if (threadIdx.x < 32) {
+            const uint32_t k = threadIdx.x;
+            GroupSlice e{};
+            uint32_t n_pos = 0, n_blk = 0;
+            if (k < count) {
+                const SliceDesc sd = d.slices[first + k];
+                const uint32_t cpm = d.frames[d.pics[sd.pic].frame].chroma == 2 ? 2u : 4u;
+                e.nb_y = 4u * sd.mbs;
+                e.nb_c = cpm * sd.mbs;
+                e.live = d.pic_status[sd.pic].locate_slice < 0;
+                n_pos = 64u * (e.nb_y + 2u * e.nb_c);
+                n_blk = e.live ? e.nb_y + 2u * e.nb_c : 0u;
+            }
+            const uint32_t ip = warp_incl_scan(n_pos), ib = warp_incl_scan(n_blk);
+            e.pos = ip - n_pos;
+            e.blk = ib - n_blk;
+            if (k < count) gs[k] = e;
+            if (k == 31) s_blocks = ib;
+        }
+        // F = QF W qScale / 8, one factor per raster position (src/decode.rs:356).
+        for (uint32_t i = threadIdx.x; i < 128u * count; i += kDecodeThreads) {
+            const uint32_t k = i >> 7, which = (i >> 6) & 1u, r = i & 63u;
+            const SliceDesc sd = d.slices[first + k];
+            const FrameDesc &fd = d.frames[d.pics[sd.pic].frame];
+            uint32_t qi = sd.size >= 2 ? d.bits[sd.off + 1] : 1u;
+            qi = qi < 1u ? 1u : (qi > 224u ? 224u : qi);
+            scale[i] = (float)((uint32_t)d.weights[fd.weights * 128u + which * 64u + r] * qscale(qi)) / 8.0f;
+        }
+        __syncthreads();
+
+        // 2. Entropy decoding, one component a thread.
+        for (uint32_t i = threadIdx.x; i < 4u * count; i += kDecodeThreads) {
+            const uint32_t c = i / count, k = i - c * count;
+            const GroupSlice e = gs[k];
+            if (!e.live) continue;  // never read: the picture failed before decoding
+            const uint32_t s = first + k;
+            const SliceDesc sd = d.slices[s];
+            const PicDesc &pd = d.pics[sd.pic];
+            const FrameDesc &fd = d.frames[pd.frame];
+            const bool has_alpha = fd.alpha_bits != 0;
+            int2 *status = d.slot_status + 4ull * s + c;
+            if (c == 3 && !has_alpha) {
+                *status = make_int2(DE_OK, 0);
+                continue;
+            }
+            uint32_t start = 0, len = 0;
+            const int2 he = component_range(d.bits + sd.off, sd.size, has_alpha, c, start, len);
+            if (he.x != DE_OK) {
+                *status = c == 0 ? he : make_int2(DE_OK, 0);
+                continue;
+            }
+            Bits b;
+            b.init(d.bits, sd.off + start, len);
+            int err;
+            if (c == 3) {
+                err = decode_alpha(b, fd, pd, sd, d.alpha);
+            } else {
+                const uint32_t nb = c == 0 ? e.nb_y : e.nb_c;
+                const uint32_t off = c == 0 ? 0u : 64u * (e.nb_y + (c - 1u) * e.nb_c);
+                SlotOut<T> out{slots + e.pos + off, wide_all + sd.coef + off};
+                err = decode_component<BookRows>(b, nb, out, run_tab, level_tab);
+            }
+            *status = make_int2(err, 0);
+        }
+        __syncthreads();
+
+        // 3. Every block: transform, convert, store.
+        const uint32_t n_blocks = s_blocks;
+        for (uint32_t bi = threadIdx.x; bi < n_blocks; bi += kDecodeThreads) {
+            uint32_t k = 0;
+            while (k + 1u < count && gs[k + 1u].blk <= bi) k++;
+            const GroupSlice e = gs[k];
+            const SliceDesc sd = d.slices[first + k];
+            const PicDesc &pd = d.pics[sd.pic];
+            const FrameDesc &fd = d.frames[pd.frame];
+            uint32_t local = bi - e.blk, c = 0, nb = e.nb_y, off = 0;
+            if (local >= e.nb_y) {
+                local -= e.nb_y;
+                c = local < e.nb_c ? 1u : 2u;
+                local -= (c - 1u) * e.nb_c;
+                nb = e.nb_c;
+                off = 64u * (e.nb_y + (c - 1u) * e.nb_c);
+            }
+            const uint32_t per_mb = c == 0 ? 4u : (fd.chroma == 2 ? 2u : 4u);
+            const uint32_t m = local / per_mb, bb = local - m * per_mb;
+            uint32_t bx, by;
+            block_xy(c, fd.chroma, sd.mb_x, sd.mb_y, m, bb, bx, by);
+            const uint32_t pw = fd.plane_w[c];
+            if (bx >= pw || by >= pd.height) continue;  // wholly outside the picture
+            uint16_t *plane =
+                fd.out_planes ? fd.out_planes + (fd.plane_off[c] - fd.plane_off[0]) : d.planes + fd.plane_off[c];
+            uint16_t *row0 = plane + (uint64_t)(pd.first_row + pd.row_step * by) * pw + bx;
+            const uint64_t pitch = (uint64_t)pd.row_step * pw;
+            const float *sc = scale + (2u * k + (c > 0 ? 1u : 0u)) * 64u;
+            const T *cs = slots + e.pos + off;
+            const int32_t *wide = wide_all + sd.coef + off;
+            const uint32_t cols = min(8u, pw - bx), rows = min(8u, pd.height - by);
+            if (pd.interlaced_scan)
+                idct_block<1>(cs, wide, nb, local, sc, fd.out_scale, fd.out_bias, fd.out_max, row0, pitch, cols, rows);
+            else
+                idct_block<0>(cs, wide, nb, local, sc, fd.out_scale, fd.out_bias, fd.out_max, row0, pitch, cols, rows);
+        }
+    }
+}
+
 constexpr int kStatusThreads = 256;
 
 __global__ void __launch_bounds__(kStatusThreads) k_status(DecodeLaunch d) {
@@ -781,8 +1072,46 @@ cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+size_t decode_smem_bytes(uint32_t group, uint32_t group_positions, uint32_t slot_bytes) {
+    return 2 * 2 * kBookEntries + sizeof(GroupSlice) * kMaxGroup + 512u * group + slot_bytes * group_positions;
+}
+
+// The most shared memory a CTA of k_decode may take (a group of 8-macroblock
+// 4:4:4 slices fills about a hundred kilobytes).
+constexpr size_t kDecodeSmemMax = 200u << 10;
+
+int decode_grid(int device, uint32_t group, uint32_t group_positions, uint32_t slot_bytes) {
+    int sms = 0, fit = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const size_t smem = decode_smem_bytes(group, group_positions, slot_bytes);
+    if (slot_bytes == 1)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_decode<int8_t>, kDecodeThreads, smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_decode<int16_t>, kDecodeThreads, smem);
+    return sms * (fit > 0 ? fit : 1);
+}
+
+cudaError_t launch_decode(const DecodeLaunch &d, int grid, cudaStream_t s) {
+    if (d.n_slices == 0) return cudaSuccess;
+    const size_t smem = decode_smem_bytes(d.group, d.group_positions, d.slot_bytes);
+    if (d.group < 1 || d.group > kMaxGroup || d.group_positions % 16u != 0 || smem > kDecodeSmemMax ||
+        (d.slot_bytes != 1 && d.slot_bytes != 2))
+        return cudaErrorInvalidValue;
+    const uint32_t groups = (d.n_slices + d.group - 1u) / d.group;
+    const int g = grid > 0 && (uint32_t)grid < groups ? grid : (int)groups;
+    if (d.slot_bytes == 1)
+        k_decode<int8_t><<<g, kDecodeThreads, smem, s>>>(d);
+    else
+        k_decode<int16_t><<<g, kDecodeThreads, smem, s>>>(d);
+    return cudaGetLastError();
+}
+
 cudaError_t configure_decode_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_idct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)idct_smem_bytes());
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_decode<int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDecodeSmemMax);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_decode<int8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDecodeSmemMax);
     if (e != cudaSuccess) return e;
     float basis[64];
     dct_basis(basis);

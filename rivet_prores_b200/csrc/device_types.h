@@ -78,8 +78,10 @@ struct PicStatus {
 
 // Constant tables the kernels read (built once per device).
 struct DeviceTables {
-    uint16_t *run_decode;    // 16 x 512
-    uint16_t *level_decode;  // 9 x 512
+    uint16_t *run_decode;    // 16 x 512: a row per run context (previousRun 0-15)
+    uint16_t *level_decode;  // 9 x 512: a row per level context (previousLevelSymbol 0-8)
+    uint16_t *run_books;     // 6 x 512: a row per distinct run codebook of Table 10
+    uint16_t *level_books;   // 6 x 512: a row per distinct level codebook of Table 11
     float *basis;            // T[x][u] at 8x + u, as the crate computes it
 };
 
@@ -91,11 +93,12 @@ struct DecodeLaunch {
     SliceDesc *slices;
     int2 *slot_status;  // 4 per slice
     PicStatus *pic_status;
-    // Decoded coefficients, per slice component: a list of 32-bit entries
-    // (scanned position << 21 | 21-bit value; larger values at the region's
-    // back, see CoefList in decode.cu) in position order, in a region of
-    // 8 bytes per position of the component; coef_count[3 s + c] says how
-    // many entries there are.
+    // 8 bytes per coefficient position of every slice component. The
+    // two-kernel decode keeps each component's coefficient list there: 32-bit
+    // entries (scanned position << 21 | 21-bit value; larger values at the
+    // region's back, see CoefList in decode.cu) in position order, with
+    // coef_count[3 s + c] entries. The fused decode keeps only values that do
+    // not fit 16 bits there, as int32 at their position (see SlotOut).
     uint64_t *coef;
     uint32_t *coef_count;
     uint16_t *planes;
@@ -104,6 +107,11 @@ struct DecodeLaunch {
     unsigned int *work_counter;
     uint32_t n_frames, n_pics, n_slices;
     uint32_t entropy_per_lane;  // slice components a lane decodes per grab of the work counter
+    // Fused decode: slices a CTA takes at once, and the coefficient
+    // positions its shared memory holds for them (group x the most any
+    // slice of the batch has).
+    uint32_t group, group_positions;
+    uint32_t slot_bytes;  // 1 or 2: bytes a coefficient takes in shared memory (int8_t or int16_t)
     DeviceTables tables;
 };
 
@@ -118,6 +126,14 @@ cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s);
 cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cudaStream_t s);
 cudaError_t launch_idct(const DecodeLaunch &d, cudaStream_t s);
 cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s);
+// The fused decode (k_decode): `grid` CTAs (0: as many as fit on the device).
+cudaError_t launch_decode(const DecodeLaunch &d, int grid, cudaStream_t s);
+// Dynamic shared memory k_decode takes for a group of `group` slices holding
+// `group_positions` coefficient positions in all, `slot_bytes` each.
+size_t decode_smem_bytes(uint32_t group, uint32_t group_positions, uint32_t slot_bytes);
+// The most CTAs of k_decode resident on `device` at that shared memory.
+int decode_grid(int device, uint32_t group, uint32_t group_positions, uint32_t slot_bytes);
+constexpr uint32_t kDecodeMaxGroup = 32;
 // The grid that keeps blocks_per_sm blocks of warps_per_block warps
 // resident on every SM (0: as many as fit).
 int entropy_grid(int device, int warps_per_block, int blocks_per_sm);

@@ -327,6 +327,8 @@ Context::~Context() {
     retired.clear();
     if (tables.run_decode) cudaFree(tables.run_decode);
     if (tables.level_decode) cudaFree(tables.level_decode);
+    if (tables.run_books) cudaFree(tables.run_books);
+    if (tables.level_books) cudaFree(tables.level_books);
     if (tables.basis) cudaFree(tables.basis);
 }
 
@@ -530,6 +532,20 @@ Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaSt
     return Status();
 }
 
+void fused_group(const DecodePlan &plan, uint32_t slot_positions, uint32_t &group, uint32_t &positions) {
+    // The most coefficient positions any slice of the batch has: 64 per
+    // block, 4 + 2 chroma blocks per macroblock, up to 2^log2_slice_mbs
+    // macroblocks (no more than the picture is wide).
+    uint32_t most = 64u * 8u;
+    for (const PicDesc &p : plan.pdesc) {
+        const uint32_t cpm = plan.fdesc[p.frame].chroma == PRORES_CHROMA_422 ? 2u : 4u;
+        const uint32_t mbs = std::min(1u << p.log2_slice_mbs, p.width_in_mb);
+        most = std::max(most, 64u * (4u + 2u * cpm) * mbs);
+    }
+    group = std::max(1u, std::min(kDecodeMaxGroup, slot_positions / most));
+    positions = group * most;
+}
+
 DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan &plan) {
     DecodeLaunch d{};
     d.bits = ws.bits.as<uint8_t>();
@@ -548,7 +564,10 @@ DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan 
     d.n_frames = (uint32_t)plan.fdesc.size();
     d.n_pics = (uint32_t)plan.pdesc.size();
     d.n_slices = plan.n_slices;
-    d.entropy_per_lane = (uint32_t)ctx.current_tuning().entropy_components_per_lane;
+    const Tuning t = ctx.current_tuning();
+    d.entropy_per_lane = (uint32_t)t.entropy_components_per_lane;
+    fused_group(plan, (uint32_t)t.decode_slot_positions, d.group, d.group_positions);
+    d.slot_bytes = (uint32_t)t.decode_slot_bytes;
     d.tables = ctx.tables;
     return d;
 }
@@ -560,10 +579,15 @@ Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaS
     if ((st = record_kernel(kt, "start", s))) return st;
     PR_CUDA(launch_locate(d, s), "k_locate");
     if ((st = record_kernel(kt, "k_locate", s))) return st;
-    PR_CUDA(launch_entropy(d, ctx.current_entropy(), s), "k_entropy");
-    if ((st = record_kernel(kt, "k_entropy", s))) return st;
-    PR_CUDA(launch_idct(d, s), "k_idct");
-    if ((st = record_kernel(kt, "k_idct", s))) return st;
+    if (ctx.current_tuning().decode_fused) {
+        PR_CUDA(launch_decode(d, decode_grid(ctx.device, d.group, d.group_positions, d.slot_bytes), s), "k_decode");
+        if ((st = record_kernel(kt, "k_decode", s))) return st;
+    } else {
+        PR_CUDA(launch_entropy(d, ctx.current_entropy(), s), "k_entropy");
+        if ((st = record_kernel(kt, "k_entropy", s))) return st;
+        PR_CUDA(launch_idct(d, s), "k_idct");
+        if ((st = record_kernel(kt, "k_idct", s))) return st;
+    }
     PR_CUDA(launch_status(d, s), "k_status");
     if ((st = record_kernel(kt, "k_status", s))) return st;
     return Status();
@@ -675,6 +699,12 @@ static Status make_tables(Context &c) {
     std::vector<uint16_t> run(kRunTableWords), level(kLevelTableWords);
     build_decode_table(run_book, 16, run.data());
     build_decode_table(level_book, 9, level.data());
+    std::vector<uint16_t> run6(kBookTableWords), level6(kBookTableWords);
+    build_book_tables(run6.data(), level6.data());
+    PR_CUDA(cudaMalloc(&c.tables.run_books, run6.size() * 2), "cudaMalloc");
+    PR_CUDA(cudaMalloc(&c.tables.level_books, level6.size() * 2), "cudaMalloc");
+    PR_CUDA(cudaMemcpy(c.tables.run_books, run6.data(), run6.size() * 2, cudaMemcpyHostToDevice), "upload");
+    PR_CUDA(cudaMemcpy(c.tables.level_books, level6.data(), level6.size() * 2, cudaMemcpyHostToDevice), "upload");
     float basis[64];
     dct_basis(basis);
     PR_CUDA(cudaMalloc(&c.tables.run_decode, run.size() * 2), "cudaMalloc");
@@ -770,6 +800,9 @@ void prores_tuning_default(prores_tuning *t) {
     t->entropy_blocks_per_sm = d.entropy_blocks_per_sm;
     t->entropy_components_per_lane = d.entropy_components_per_lane;
     t->staging_depth = d.staging_depth;
+    t->decode_fused = d.decode_fused;
+    t->decode_slot_positions = d.decode_slot_positions;
+    t->decode_slot_bytes = d.decode_slot_bytes;
 }
 
 int prores_set_tuning(prores_ctx *ctx, const prores_tuning *t) {
@@ -778,13 +811,16 @@ int prores_set_tuning(prores_ctx *ctx, const prores_tuning *t) {
         t->entropy_blocks_per_sm < 0 || t->entropy_blocks_per_sm > 32 ||
         !(t->entropy_components_per_lane == 1 || t->entropy_components_per_lane == 2 ||
           t->entropy_components_per_lane == 4) ||
-        t->staging_depth < 1 || t->staging_depth > 64)
+        t->staging_depth < 1 || t->staging_depth > 64 || t->decode_fused < 0 || t->decode_fused > 1 ||
+        t->decode_slot_positions < 512 || t->decode_slot_positions > 65536 ||
+        (t->decode_slot_bytes != 1 && t->decode_slot_bytes != 2))
         return fail(make_status(PRORES_CONFIG, "tuning value out of range"));
     cudaSetDevice(ctx->impl.device);
     const int grid = entropy_grid(ctx->impl.device, t->entropy_warps_per_block, t->entropy_blocks_per_sm);
     std::lock_guard<std::mutex> g(ctx->impl.m);
     ctx->impl.tuning = Tuning{t->cost_lane_items_per_sm, t->entropy_warps_per_block, t->entropy_blocks_per_sm,
-                              t->entropy_components_per_lane, t->staging_depth};
+                              t->entropy_components_per_lane, t->staging_depth, t->decode_fused,
+                              t->decode_slot_positions, t->decode_slot_bytes};
     ctx->impl.entropy = EntropyShape{t->entropy_warps_per_block, grid};
     return PRORES_OK;
 }
@@ -797,6 +833,9 @@ int prores_get_tuning(prores_ctx *ctx, prores_tuning *t) {
     t->entropy_blocks_per_sm = c.entropy_blocks_per_sm;
     t->entropy_components_per_lane = c.entropy_components_per_lane;
     t->staging_depth = c.staging_depth;
+    t->decode_fused = c.decode_fused;
+    t->decode_slot_positions = c.decode_slot_positions;
+    t->decode_slot_bytes = c.decode_slot_bytes;
     return PRORES_OK;
 }
 

@@ -118,6 +118,9 @@ struct Tuning {
     int entropy_blocks_per_sm = 0;
     int entropy_components_per_lane = 1;
     int staging_depth = 4;
+    int decode_fused = 1;               // one kernel for the per-slice decode (else entropy, then IDCT)
+    int decode_slot_positions = 16384;  // coefficient positions a CTA of the fused decode holds
+    int decode_slot_bytes = 2;          // bytes a coefficient takes there (1: int8, 2: int16)
 };
 
 struct Context {
@@ -193,6 +196,9 @@ Status plan_decode(const prores_buf *in, int n, uint32_t out_depth, DecodePlan &
 Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s);
 Status upload_decode_bits(Workspace &ws, const DecodePlan &plan, const prores_buf *in, cudaStream_t s);
 DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan &plan);
+// The fused decode's group: slices a CTA takes at once, and the coefficient
+// positions it holds for them, for CTAs of at most `slot_positions`.
+void fused_group(const DecodePlan &plan, uint32_t slot_positions, uint32_t &group, uint32_t &positions);
 Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s, KernelTimes *kt);
 Status fetch_decode(Workspace &ws, const DecodePlan &plan, cudaStream_t s, prores_frame *out, int *status,
                     Status *first_err, bool device_out = false);

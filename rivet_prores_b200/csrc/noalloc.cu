@@ -7,15 +7,18 @@
 // accounting or fails outright. prores_decode_noalloc serves them. The
 // caller passes the frame's bytes and device buffers for the planes; all
 // the decoder's scratch (its tables, the frame and slice descriptors, a
-// copy of the bitstream, the coefficient lists and statuses) lives in one
+// copy of the bitstream, the statuses, and room for the rare coefficient
+// too wide for the kernel's 16-bit shared-memory slots) lives in one
 // static device array of PRORES_NOALLOC_SCRATCH_BYTES, which every GPU that
 // loads this part of the library holds until the process exits.
 //
-// The kernels are the ones every other decode runs (decode.cu); only where
+// The kernels are the ones every other decode runs (decode.cu: the slice
+// table scan, the fused per-slice decode, the status reduction); only where
 // their scratch lives differs.
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -35,13 +38,12 @@ namespace {
 static __device__ __align__(256) unsigned char g_scratch[PRORES_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-constexpr size_t kTablesBytes = 32 << 10;  // run and level prefix tables, the DCT basis
+constexpr size_t kTablesBytes = 16 << 10;  // the run and level prefix tables (a row per codebook)
 constexpr size_t kDescBytes = 4 << 10;     // frame and picture descriptors, statuses, weights, counter
 
 struct DeviceSetup {
     bool done = false;
     unsigned char *base = nullptr;  // device address of g_scratch on this device
-    EntropyShape entropy{8, 0};  // the library's default shape
 };
 
 std::mutex g_lock;
@@ -61,24 +63,13 @@ Status setup(int device, DeviceSetup **out) {
         if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress of the no-allocation scratch");
         e = configure_decode_kernels();
         if (e != cudaSuccess) return cuda_status(e, "configure decode kernels");
-        static uint16_t run[kRunTableWords], level[kLevelTableWords];
-        static float basis[64];
-        build_decode_table(run_book, 16, run);
-        build_decode_table(level_book, 9, level);
-        for (int x = 0; x < 8; x++)
-            for (int u = 0; u < 8; u++) {
-                const double cu = u == 0 ? 0.70710678118654752440 : 1.0;
-                const double a = (double)((2 * x + 1) * u) * 3.14159265358979323846 / 16.0;
-                basis[8 * x + u] = (float)(cu / 2.0 * cos(a));
-            }
+        static uint16_t run[kBookTableWords], level[kBookTableWords];
+        build_book_tables(run, level);
         unsigned char *base = static_cast<unsigned char *>(ptr);
         if ((e = cudaMemcpy(base, run, sizeof run, cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMemcpy(base + sizeof run, level, sizeof level, cudaMemcpyHostToDevice)) != cudaSuccess ||
-            (e = cudaMemcpy(base + sizeof run + sizeof level, basis, sizeof basis, cudaMemcpyHostToDevice)) !=
-                cudaSuccess)
+            (e = cudaMemcpy(base + sizeof run, level, sizeof level, cudaMemcpyHostToDevice)) != cudaSuccess)
             return cuda_status(e, "upload of the decode tables");
         d.base = base;
-        d.entropy = EntropyShape{8, entropy_grid(device, 8, 0)};
         d.done = true;
     }
     *out = &d;
@@ -162,6 +153,7 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
     PicDesc pics[2]{};
     uint32_t n_pics = 0, n_slices = 0;
     uint64_t coef_total = 0;
+    uint32_t most = 64u * 8u;  // the most coefficient positions of any slice
     Status late;
     const uint32_t cpm = h.chroma == PRORES_CHROMA_422 ? 2u : 4u;
     const uint32_t width_in_mb = (h.width + 15u) / 16u;
@@ -198,6 +190,7 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
         p.interlaced_scan = h.interlace != 0;
         n_slices += (uint32_t)ns;
         coef_total += (uint64_t)width_in_mb * height_in_mb * 64u * (4u + 2u * cpm);
+        most = std::max(most, 64u * (4u + 2u * cpm) * std::min(1u << ph.log2_slice_mbs, width_in_mb));
         n_pics++;
         pos += ph.picture_size;
     }
@@ -206,14 +199,13 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
     const size_t o_desc = kTablesBytes;
     const size_t o_slices = o_desc + kDescBytes;
     const size_t o_slots = o_slices + align256(sizeof(SliceDesc) * ((size_t)n_slices + 1));
-    const size_t o_counts = o_slots + align256(sizeof(int2) * 4 * ((size_t)n_slices + 1));
-    const size_t o_bits = o_counts + align256(4 * 3 * ((size_t)n_slices + 1));
-    const size_t o_coef = o_bits + align256((size_t)h.frame_size + 64);
-    const size_t need = o_coef + 8 * (size_t)coef_total;
+    const size_t o_bits = o_slots + align256(sizeof(int2) * 4 * ((size_t)n_slices + 1));
+    const size_t o_wide = o_bits + align256((size_t)h.frame_size + 64);
+    const size_t need = o_wide + 4 * (size_t)coef_total;
     if (need > PRORES_NOALLOC_SCRATCH_BYTES)
         return finish(make_status(
             PRORES_CONFIG, strf("a %u\xc3\x97%u frame needs %zu bytes of decoder scratch; prores_decode_noalloc has "
-                                "%u (frames up to 1920\xc3\x97" "1080)",
+                                "%u (4 bytes a coefficient position, the frame's bytes and 64 a slice)",
                                 h.width, h.height, need, (unsigned)PRORES_NOALLOC_SCRATCH_BYTES)));
 
     unsigned char *base = dev->base;
@@ -242,8 +234,8 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
     d.slices = reinterpret_cast<SliceDesc *>(base + o_slices);
     d.slot_status = reinterpret_cast<int2 *>(base + o_slots);
     d.pic_status = d_status;
-    d.coef = reinterpret_cast<uint64_t *>(base + o_coef);
-    d.coef_count = reinterpret_cast<uint32_t *>(base + o_counts);
+    d.coef = reinterpret_cast<uint64_t *>(base + o_wide);  // values past 16 bits, at their positions
+    d.coef_count = nullptr;
     d.planes = d_planes;
     d.alpha = d_alpha;
     d.weights = d_weights;
@@ -252,11 +244,14 @@ extern "C" int prores_decode_noalloc(int device, const uint8_t *data, size_t len
     d.n_pics = n_pics;
     d.n_slices = n_slices;
     d.entropy_per_lane = 1;
-    d.tables.run_decode = reinterpret_cast<uint16_t *>(base);
-    d.tables.level_decode = reinterpret_cast<uint16_t *>(base + 2 * kRunTableWords);
-    d.tables.basis = reinterpret_cast<float *>(base + 2 * (kRunTableWords + kLevelTableWords));
-    if ((e = launch_locate(d, s)) != cudaSuccess || (e = launch_entropy(d, dev->entropy, s)) != cudaSuccess ||
-        (e = launch_idct(d, s)) != cudaSuccess || (e = launch_status(d, s)) != cudaSuccess)
+    d.group = std::max(1u, std::min(kDecodeMaxGroup, 16384u / most));
+    d.group_positions = d.group * most;
+    d.slot_bytes = 2;
+    d.tables.run_books = reinterpret_cast<uint16_t *>(base);
+    d.tables.level_books = reinterpret_cast<uint16_t *>(base + 2 * kBookTableWords);
+    if ((e = launch_locate(d, s)) != cudaSuccess ||
+        (e = launch_decode(d, decode_grid(device, d.group, d.group_positions, d.slot_bytes), s)) != cudaSuccess ||
+        (e = launch_status(d, s)) != cudaSuccess)
         return finish(cuda_status(e, "decode launch"));
     PicStatus ps[2]{};
     if (n_pics && (e = cudaMemcpyAsync(ps, d_status, sizeof(PicStatus) * n_pics, cudaMemcpyDeviceToHost, s)) !=

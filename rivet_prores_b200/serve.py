@@ -24,7 +24,7 @@ import threading
 import time
 from concurrent.futures import Future
 from dataclasses import dataclass, field
-from typing import Callable, Deque, List, Optional
+from typing import Callable, Deque, Dict, List, Optional
 
 import numpy as np
 
@@ -189,7 +189,10 @@ class Server:
         self.budget = memory_budget
         self.max_batch = max_batch
         self.in_use = 0
-        self.queue: Deque[Request] = collections.deque()
+        # One first-in-first-out queue per kind: taking a batch pops from the
+        # front of one of them, whatever is waiting behind.
+        self.queues: Dict[str, Deque[Request]] = {"decode": collections.deque(), "encode": collections.deque()}
+        self.waiting = 0
         self.cv = threading.Condition()
         self.closed = False
         # (submitted, done) times of finished requests: the requests
@@ -225,9 +228,10 @@ class Server:
         with self.cv:
             if self.closed:
                 raise RuntimeError("server closed")
-            self.queue.append(r)
-            self.peak_queue = max(self.peak_queue, len(self.queue))
-            self.cv.notify_all()
+            self.queues[r.kind].append(r)
+            self.waiting += 1
+            self.peak_queue = max(self.peak_queue, self.waiting)
+            self.cv.notify()
         return r.future
 
     # -------------------------------------------------------------- batching
@@ -236,20 +240,17 @@ class Server:
         """Under the lock: the oldest request's kind, and further requests of
         that kind oldest first, while the budget admits them. A request larger
         than the whole budget runs alone once nothing else is in flight."""
-        head = self.queue[0]
+        heads = [q for q in self.queues.values() if q]
+        q = min(heads, key=lambda d: d[0].t_submit)
         batch, cost = [], 0
         free = self.budget - self.in_use
-        for r in list(self.queue):
-            if r.kind != head.kind:
-                continue
-            if len(batch) >= self.max_batch:
-                break
+        while q and len(batch) < self.max_batch:
+            r = q[0]
             if cost + r.cost > free and not (not batch and self.in_use == 0):
                 break
-            batch.append(r)
+            batch.append(q.popleft())
             cost += r.cost
-        for r in batch:
-            self.queue.remove(r)
+        self.waiting -= len(batch)
         self.in_use += cost
         self.peak_in_use = max(self.peak_in_use, self.in_use)
         return batch
@@ -258,9 +259,9 @@ class Server:
         while True:
             with self.cv:
                 while True:
-                    if self.closed and not self.queue:
+                    if self.closed and not self.waiting:
                         return
-                    if self.queue:
+                    if self.waiting:
                         batch = self._take()
                         if batch:
                             break

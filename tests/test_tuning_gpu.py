@@ -14,11 +14,17 @@ pytestmark = pytest.mark.gpu
 SHAPES = [
     P.Tuning(),
     P.Tuning(cost_lane_items_per_sm=0, entropy_warps_per_block=1, entropy_blocks_per_sm=1,
-             entropy_components_per_lane=4, staging_depth=1),
+             entropy_components_per_lane=4, staging_depth=1, decode_fused=0),
     P.Tuning(cost_lane_items_per_sm=1 << 30, entropy_warps_per_block=16, entropy_blocks_per_sm=0,
-             entropy_components_per_lane=2, staging_depth=64),
+             entropy_components_per_lane=2, staging_depth=64, decode_fused=0),
     P.Tuning(cost_lane_items_per_sm=0, entropy_warps_per_block=3, entropy_blocks_per_sm=2,
-             entropy_components_per_lane=1, staging_depth=3),
+             entropy_components_per_lane=1, staging_depth=3, decode_fused=0),
+    # The fused decoder from one slice a CTA up to the most its shared memory takes.
+    P.Tuning(decode_slot_positions=512),
+    P.Tuning(decode_slot_positions=6144),
+    P.Tuning(decode_slot_positions=65536),
+    P.Tuning(decode_slot_positions=512, decode_slot_bytes=1),
+    P.Tuning(decode_slot_positions=65536, decode_slot_bytes=1),
 ]
 
 
@@ -67,7 +73,9 @@ def test_out_of_range_tunings_are_refused():
     ctx = P.context(0)
     saved = ctx.tuning
     for bad in [dict(entropy_warps_per_block=0), dict(entropy_warps_per_block=17), dict(entropy_components_per_lane=3),
-                dict(staging_depth=0), dict(cost_lane_items_per_sm=-1), dict(entropy_blocks_per_sm=-1)]:
+                dict(staging_depth=0), dict(cost_lane_items_per_sm=-1), dict(entropy_blocks_per_sm=-1),
+                dict(decode_fused=2), dict(decode_slot_positions=511), dict(decode_slot_positions=65537),
+                dict(decode_slot_bytes=3)]:
         with pytest.raises(P.Error.Config):
             ctx.set_tuning(P.Tuning(**bad))
     assert ctx.tuning == saved
@@ -84,6 +92,6 @@ def test_quick_autotune_applies_a_valid_tuning(tmp_path, monkeypatch):
         t, ev = autotune.tune(quick=True, frames=frames, depths=[2, 4])
         assert ctx.tuning == t
         assert autotune.load() == t
-        assert {"cost", "entropy", "staging"} <= set(ev)
+        assert {"cost", "decode", "staging"} <= set(ev)
     finally:
         ctx.set_tuning(saved)

@@ -39,6 +39,20 @@ def _packets():
     return [hd_pkt, small_pkt]
 
 
+def _device_memory():
+    """(free bytes on the device, bytes the device's default memory pool has
+    reserved): what any device allocation would change."""
+    import torch
+
+    rt = ctypes.CDLL("libcudart.so.12")
+    pool = ctypes.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), 0) == 0
+    reserved = ctypes.c_uint64()
+    assert rt.cudaMemPoolGetAttribute(pool, 5, ctypes.byref(reserved)) == 0  # cudaMemPoolAttrReservedMemCurrent
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info(0)[0], reserved.value
+
+
 def test_decode_without_allocation_equals_the_allocating_decode():
     import torch
 
@@ -52,6 +66,18 @@ def test_decode_without_allocation_equals_the_allocating_decode():
         planes = torch.empty(info.data_len, dtype=torch.int16, device="cuda")
         alpha = torch.empty(max(info.alpha_len, 1), dtype=torch.int16, device="cuda")
         outs.append((info, planes, alpha))
+    # One call first (it sets the device up and loads the kernels), and
+    # everything else the loop below runs once (torch loads its kernels on
+    # first use too); from then on nothing may change what the device has
+    # allocated.
+    for info, planes, alpha in outs:
+        planes.fill_(-1)
+        alpha.fill_(-1)
+        planes.cpu()
+        alpha.cpu()
+    info, planes, alpha = outs[0]
+    assert decode(0, packets[0], len(packets[0]), 0, planes.data_ptr(), info.data_len, None, 0, None) == _abi.OK
+    before = _device_memory()
     # Two calls in a row on each frame, then the frames interleaved: every
     # call shares the scratch the previous call left behind.
     for i in [0, 0, 1, 1, 0, 1]:
@@ -66,6 +92,7 @@ def test_decode_without_allocation_equals_the_allocating_decode():
         assert np.array_equal(got, wants[i].data), f"frame {i}"
         if info.alpha_len:
             assert np.array_equal(alpha.cpu().numpy().view(np.uint16)[: info.alpha_len], wants[i].alpha)
+    assert _device_memory() == before, "a call allocated device memory"
 
 
 def test_frames_beyond_the_scratch_are_refused():
