@@ -54,6 +54,13 @@ KERNEL_BYTES = {
     "k_entropy": (lambda s, p: p, "packet in (coefficient lists are an intermediate)"),
     "k_idct": (lambda s, p: 2 * s, "u16 planes out (coefficient lists are an intermediate)"),
 }
+# What the CPU codec timed beside the GPU is, and what the crate itself
+# publishes for the same work on other hardware.
+CPU_CODE = ("the oracle's scalar restatement of the crate's CPU path, with its slice-parallel pool (no hand-written "
+            "SIMD; the crate's SIMD levels give bit-identical output, so this is a slower, equal-output stand-in), "
+            "compiled -O3 -march=x86-64-v3 -ffp-contract=off")
+PUBLISHED_CRATE = ("the crate's README: 1920x1080 422 HQ at 296 encode / 907 decode frames/s on 32 threads of a Ryzen 9 "
+                   "9950X, about 74 / 227 at UHD (4x the samples), about 56 round trips/s; other hardware")
 # Figures from ncu captures of these kernels, not measured by this run: the
 # capture's DRAM bytes (read + write) per frame and launch, and issue-slot use.
 CAPTURED = {
@@ -205,10 +212,7 @@ def cpu_baseline(frames, cfg):
             "sample": f"UHD 422 HQ frames: encode and decode timed separately, best of 5, pictures prepared "
                       f"outside the timed region; {n_all} frames on all {cores} host threads, 1 frame on 1 thread; "
                       f"`value` is the round trip (1 / (1/encode + 1/decode)) on all threads",
-            "code": "the oracle's scalar restatement of the crate's CPU path (no hand-written SIMD; the crate's "
-                    "SIMD levels give bit-identical output), compiled -O3 -march=x86-64-v3 -ffp-contract=off",
-            "published_crate": "README.md: 1920x1080 422 HQ 296 encode / 907 decode frames/s on 32 threads of a "
-                               "Ryzen 9 9950X, i.e. about 74 / 227 at UHD (4x the samples); other hardware"}
+            "code": CPU_CODE, "published_crate": PUBLISHED_CRATE}
 
 
 def run_reference(args):
@@ -248,7 +252,7 @@ def run_reference(args):
                    "chroma": "4:2:2", "bit_depth": 10, "profile": "HQ (apch)",
                    "step": "encode each frame, then decode its packet"},
         "cpu_baseline": {"value": round(fps, 3), "unit": "frames/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "code": CPU_CODE, "published_crate": PUBLISHED_CRATE},
         "e2e": {"value": round(fps, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

@@ -351,8 +351,8 @@ class Tuning:
     entropy_components_per_lane: int = 1
     staging_depth: int = 4
     decode_fused: int = 1
-    decode_slot_positions: int = 16384
-    decode_slot_bytes: int = 2
+    decode_slot_positions: int = 65536
+    decode_slot_bytes: int = 1
 
     def _c(self) -> "_abi.Tuning_":
         t = _abi.Tuning_()

@@ -114,10 +114,13 @@ def lib():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
+    # RIVET_PRORES_LIB names another build of the same library (to compare
+    # builds side by side); by default the in-tree one.
+    path = os.environ.get("RIVET_PRORES_LIB") or LIB_PATH
+    if not os.path.exists(path):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python rivet_prores_b200/build.py` (nvcc, sm_100a)")
-    L = ctypes.CDLL(LIB_PATH)
+            f"{path} is missing: build it with `python rivet_prores_b200/build.py` (nvcc, sm_100a)")
+    L = ctypes.CDLL(path)
     vp = ctypes.c_void_p
     sig = {
         "prores_create": (vp, [ctypes.c_int]),

@@ -202,7 +202,7 @@ def tune(device: int = 0, quick: bool = False, store: bool = True, frames: Optio
     shapes = {}
     # The fused decoder by slice group size ...
     for nbytes in (1, 2):
-        for pos in ([8192, 16384, 32768] if quick else [4096, 8192, 12288, 16384, 24576, 32768, 49152]):
+        for pos in ([16384, 32768, 65536] if quick else [8192, 16384, 24576, 32768, 49152, 65536]):
             ctx.set_tuning(type(tuning)(**{**asdict(tuning), "decode_fused": 1, "decode_slot_positions": pos,
                                            "decode_slot_bytes": nbytes}))
             shapes[(1, pos, nbytes, 0, 0, 0)] = _time(lambda: dec.launch(stream), stream, reps)

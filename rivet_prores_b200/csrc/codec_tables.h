@@ -152,16 +152,41 @@ inline void build_decode_table(Books books, int n_books, uint16_t *out) {
     }
 }
 
-// One row per distinct codebook, for decoders that map a context to its
-// codebook: Table 10's run codebooks for previousRun 0-1, 2-3, 4, 5-8, 9-14,
-// 15+ and Table 11's level codebooks for previousLevelSymbol 0, 1, 2, 3,
-// 4-7, 8+ (the first context of each range stands for it).
+// One row per distinct codebook: Table 10's run codebooks for previousRun
+// 0-1, 2-3, 4, 5-8, 9-14, 15+ (rows 0-5) and Table 11's level codebooks for
+// previousLevelSymbol 0, 1, 2, 3, 4-7, 8+ (rows 0-5). For every 9-bit window
+// prefix an entry holds the codeword it starts with when that is 9 bits or
+// fewer: its length (4 bits), its symbol (6 bits: every such symbol is below
+// 64) and the row the next code of the same kind is read with, the row of
+// the context this symbol makes (3 bits); 0 when the codeword is longer.
 static constexpr uint32_t kBookTableWords = 6 * kDecodeEntries;
+
+PR_HD uint32_t run_book_row(uint32_t prev_run) {
+    return (uint32_t)(0x5444444333321100ull >> (4u * (prev_run < 15u ? prev_run : 15u))) & 15u;
+}
+PR_HD uint32_t level_book_row(uint32_t prev_level) {
+    return (uint32_t)(0x544443210ull >> (4u * (prev_level < 8u ? prev_level : 8u))) & 15u;
+}
+
 inline void build_book_tables(uint16_t *run, uint16_t *level) {
     static const uint32_t run_ctx[6] = {0, 2, 4, 5, 9, 15};
     static const uint32_t level_ctx[6] = {0, 1, 2, 3, 4, 8};
-    build_decode_table([&](uint32_t i) { return run_book(run_ctx[i]); }, 6, run);
-    build_decode_table([&](uint32_t i) { return level_book(level_ctx[i]); }, 6, level);
+    for (int kind = 0; kind < 2; kind++) {
+        uint16_t *out = kind == 0 ? run : level;
+        for (uint32_t row = 0; row < 6; row++) {
+            const Codebook cb = kind == 0 ? run_book(run_ctx[row]) : level_book(level_ctx[row]);
+            uint16_t *r = out + row * kDecodeEntries;
+            for (uint32_t i = 0; i < kDecodeEntries; i++) r[i] = 0;
+            for (uint32_t n = 0; n < 64; n++) {
+                const uint32_t len = cb_len(cb, n);
+                if (len > kDecodeBits) continue;
+                const uint32_t next = kind == 0 ? run_book_row(n) : level_book_row(n);
+                const uint32_t first = (uint32_t)cb_bits(cb, n) << (kDecodeBits - len);
+                for (uint32_t p = 0; p < (1u << (kDecodeBits - len)); p++)
+                    r[first + p] = (uint16_t)(len | (n << 4) | (next << 10));
+            }
+        }
+    }
 }
 
 }  // namespace prores

@@ -190,28 +190,53 @@ __device__ __forceinline__ void list_entry(const uint32_t *w, uint32_t cap, uint
     if (v < kListMin) v = (int32_t)__ldg(w + 2u * cap - 1u - (uint32_t)(v + (1 << 20)));
 }
 
-// Prefix-table rows by context: the rows of `run_tab` and `level_tab` are
-// either one per context (16 run, 9 level contexts) or one per distinct
-// codebook (Tables 10 and 11 have 6 each), as `Rows` says.
-struct ContextRows {
-    __device__ __forceinline__ static uint32_t run(uint32_t ctx) { return ctx < 15u ? ctx : 15u; }
-    __device__ __forceinline__ static uint32_t level(uint32_t ctx) { return ctx < 8u ? ctx : 8u; }
-};
-struct BookRows {
-    // Table 10: previousRun 0-1, 2-3, 4, 5-8, 9-14, 15+ share a codebook;
-    // Table 11: previousLevelSymbol 0, 1, 2, 3, 4-7, 8+.
-    __device__ __forceinline__ static uint32_t run(uint32_t ctx) {
-        return (uint32_t)(0x5444444333321100ull >> (4u * (ctx < 15u ? ctx : 15u))) & 15u;
+// The read position as a 64-bit window consumed from the top: `cur` holds
+// the bits [pos, pos + avail) MSB first with zeros below, and is refilled
+// 32 bits at a time from big-endian words fetched one word ahead, so that a
+// symbol costs shifts of the window rather than a fresh funnel shift of two
+// words. Reads the same bits as Bits; only used while at least 32 bits of
+// the component remain, so the top 32 bits are always data.
+struct Window {
+    const uint32_t *w;
+    uint64_t cur;
+    uint32_t avail, left;  // valid bits in cur (>= 32); bits of the component from pos on
+    uint64_t next;         // index of the word after those in cur
+    uint32_t nxt;          // that word
+
+    __device__ __forceinline__ static uint32_t be32(uint32_t v) { return __byte_perm(v, 0, 0x0123); }
+    __device__ __forceinline__ void init(const uint8_t *base, uint64_t pos, uint64_t end) {
+        w = reinterpret_cast<const uint32_t *>(base);
+        const uint64_t i = pos >> 5;
+        const uint32_t skip = (uint32_t)(pos & 31);
+        cur = (((uint64_t)be32(__ldg(w + i)) << 32) | be32(__ldg(w + i + 1))) << skip;
+        avail = 64u - skip;
+        next = i + 2;
+        nxt = be32(__ldg(w + next));
+        left = (uint32_t)(end - pos);
     }
-    __device__ __forceinline__ static uint32_t level(uint32_t ctx) {
-        return (uint32_t)(0x544443210ull >> (4u * (ctx < 8u ? ctx : 8u))) & 15u;
+    __device__ __forceinline__ uint32_t top() const { return (uint32_t)(cur >> 32); }
+    __device__ __forceinline__ void consume(uint32_t len) {
+        cur <<= len;
+        avail -= len;
+        left -= len;
+        if (avail < 32u) {
+            cur |= (uint64_t)nxt << (32u - avail);
+            avail += 32u;
+            nxt = be32(__ldg(w + ++next));
+        }
     }
 };
 
 // scanned_coefficients() of one component (src/decode.rs:484-540): every
 // coefficient the codes give, in scanned-index order, handed to `out.put`
-// (position, value); the positions not handed over are zero.
-template <class Rows = ContextRows, class Out>
+// (position, value); the positions not handed over are zero. `run_tab` and
+// `level_tab` are the packed prefix tables of build_book_tables (a row per
+// distinct codebook): while 32 or more bits remain, a run, level and sign
+// whose codewords are both in them are read from the window in one go (all
+// the bits they take are data, and the tables give the symbols the general
+// reader would); anything else, and the end of the data, goes through the
+// general reader, which also names every failure as the crate does.
+template <class Out>
 __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
     uint32_t sym;
@@ -233,41 +258,38 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
     const uint32_t total = n_blocks * 64;
     uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
     for (;;) {
-        uint64_t rem = b.remaining();
-        uint64_t w = b.peek();
-        if (rem >= 64) {
-            // Run, level and sign from one window when both codewords are
-            // in the prefix tables (all 64 window bits are data here).
-            uint32_t e1 = run_tab[Rows::run(prev_run) * kDecodeEntries + (w >> (64 - kDecodeBits))];
-            if (e1) {
-                uint32_t l1 = e1 & 31;
-                uint64_t w2 = w << l1;
-                uint32_t e2 = level_tab[Rows::level(prev_level) * kDecodeEntries + (w2 >> (64 - kDecodeBits))];
-                if (e2) {
-                    uint32_t l2 = e2 & 31;
-                    uint32_t run = e1 >> 5, lvl = e2 >> 5;
-                    n += run;
-                    if (n >= total) return DE_RUN_PAST_END;
-                    int32_t level = (int32_t)lvl + 1;
-                    bool neg = (w2 << l2) >> 63;
-                    b.pos += l1 + l2 + 1;
-                    out.put(n, neg ? -level : level);
-                    n += 1;
-                    prev_run = run;
-                    prev_level = lvl;
-                    continue;
-                }
+        if (b.remaining() >= 32) {
+            Window win;
+            win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
+            uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
+            while (win.left >= 32u) {
+                const uint32_t t = win.top();
+                const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
+                if (!e1) break;
+                const uint32_t l1 = e1 & 15u, t2 = t << l1;
+                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
+                if (!e2) break;
+                const uint32_t l2 = e2 & 15u;
+                prev_run = (e1 >> 4) & 63u;
+                prev_level = (e2 >> 4) & 63u;
+                n += prev_run;
+                if (n >= total) return DE_RUN_PAST_END;
+                const int32_t level = (int32_t)prev_level + 1;
+                out.put(n, (t2 << l2) >> 31 ? -level : level);
+                n += 1;
+                rrow = (e1 >> 10) * kDecodeEntries;
+                lrow = (e2 >> 10) * kDecodeEntries;
+                win.consume(l1 + l2 + 1u);
             }
-        } else if (rem <= 31 && w == 0) {
-            break;  // endOfData()
+            b.pos = b.end - win.left;
         }
+        if (b.remaining() <= 31 && b.peek() == 0) break;  // endOfData()
         uint32_t run, lvl;
-        if ((err = read_sym(b, run_tab + Rows::run(prev_run) * kDecodeEntries, run_book(prev_run), run))) return err;
+        if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return err;
         prev_run = run;
         n += run;
         if (n >= total) return DE_RUN_PAST_END;
-        if ((err = read_sym(b, level_tab + Rows::level(prev_level) * kDecodeEntries, level_book(prev_level), lvl)))
-            return err;
+        if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return err;
         prev_level = lvl;
         if (b.remaining() < 1) return DE_PAST_END;
         bool neg = b.peek() >> 63;
@@ -519,12 +541,12 @@ constexpr int kEntropyMaxThreads = 512;
 // grab of the work counter, a lane each in turn, component-major, until the
 // list runs out.
 __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) {
-    __shared__ uint16_t run_tab[kRunTableWords];
-    __shared__ uint16_t level_tab[kLevelTableWords];
-    for (uint32_t i = threadIdx.x; i < kRunTableWords / 2; i += blockDim.x)
-        reinterpret_cast<uint32_t *>(run_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.run_decode)[i];
-    for (uint32_t i = threadIdx.x; i < kLevelTableWords / 2; i += blockDim.x)
-        reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_decode)[i];
+    __shared__ uint16_t run_tab[kBookTableWords];
+    __shared__ uint16_t level_tab[kBookTableWords];
+    for (uint32_t i = threadIdx.x; i < kBookTableWords / 2; i += blockDim.x) {
+        reinterpret_cast<uint32_t *>(run_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.run_books)[i];
+        reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_books)[i];
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint32_t items = 4u * d.n_slices;
@@ -934,39 +956,49 @@ __global__ void __launch_bounds__(kDecodeThreads) k_decode(DecodeLaunch d) {
         }
         __syncthreads();
 
-        // 2. Entropy decoding, one component a thread.
+        // 2. Entropy decoding. Thread i takes item kind i / count of slice
+        // i % count: kind 0 its Y', kind 1 its Cb and then its Cr for 4:2:2
+        // (together about as long as Y') or its Cb for 4:4:4, kind 2 the
+        // Cr of a 4:4:4 slice, kind 3 its alpha; so the threads of a warp
+        // mostly decode codes of about equal length.
         for (uint32_t i = threadIdx.x; i < 4u * count; i += kDecodeThreads) {
-            const uint32_t c = i / count, k = i - c * count;
+            const uint32_t kind = i / count, k = i - kind * count;
             const GroupSlice e = gs[k];
             if (!e.live) continue;  // never read: the picture failed before decoding
             const uint32_t s = first + k;
             const SliceDesc sd = d.slices[s];
             const PicDesc &pd = d.pics[sd.pic];
             const FrameDesc &fd = d.frames[pd.frame];
-            const bool has_alpha = fd.alpha_bits != 0;
-            int2 *status = d.slot_status + 4ull * s + c;
-            if (c == 3 && !has_alpha) {
-                *status = make_int2(DE_OK, 0);
-                continue;
+            const bool pair = fd.chroma == 2;  // 4:2:2: Cb and Cr on one thread
+            uint32_t c = kind, last = kind;
+            if (kind == 1 && pair) last = 2;
+            if (kind == 2 && pair) continue;
+            for (; c <= last; c++) {
+                const bool has_alpha = fd.alpha_bits != 0;
+                int2 *status = d.slot_status + 4ull * s + c;
+                if (c == 3 && !has_alpha) {
+                    *status = make_int2(DE_OK, 0);
+                    continue;
+                }
+                uint32_t start = 0, len = 0;
+                const int2 he = component_range(d.bits + sd.off, sd.size, has_alpha, c, start, len);
+                if (he.x != DE_OK) {
+                    *status = c == 0 ? he : make_int2(DE_OK, 0);
+                    continue;
+                }
+                Bits b;
+                b.init(d.bits, sd.off + start, len);
+                int err;
+                if (c == 3) {
+                    err = decode_alpha(b, fd, pd, sd, d.alpha);
+                } else {
+                    const uint32_t nb = c == 0 ? e.nb_y : e.nb_c;
+                    const uint32_t off = c == 0 ? 0u : 64u * (e.nb_y + (c - 1u) * e.nb_c);
+                    SlotOut<T> out{slots + e.pos + off, wide_all + sd.coef + off};
+                    err = decode_component(b, nb, out, run_tab, level_tab);
+                }
+                *status = make_int2(err, 0);
             }
-            uint32_t start = 0, len = 0;
-            const int2 he = component_range(d.bits + sd.off, sd.size, has_alpha, c, start, len);
-            if (he.x != DE_OK) {
-                *status = c == 0 ? he : make_int2(DE_OK, 0);
-                continue;
-            }
-            Bits b;
-            b.init(d.bits, sd.off + start, len);
-            int err;
-            if (c == 3) {
-                err = decode_alpha(b, fd, pd, sd, d.alpha);
-            } else {
-                const uint32_t nb = c == 0 ? e.nb_y : e.nb_c;
-                const uint32_t off = c == 0 ? 0u : 64u * (e.nb_y + (c - 1u) * e.nb_c);
-                SlotOut<T> out{slots + e.pos + off, wide_all + sd.coef + off};
-                err = decode_component<BookRows>(b, nb, out, run_tab, level_tab);
-            }
-            *status = make_int2(err, 0);
         }
         __syncthreads();
 

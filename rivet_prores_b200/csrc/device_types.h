@@ -78,10 +78,8 @@ struct PicStatus {
 
 // Constant tables the kernels read (built once per device).
 struct DeviceTables {
-    uint16_t *run_decode;    // 16 x 512: a row per run context (previousRun 0-15)
-    uint16_t *level_decode;  // 9 x 512: a row per level context (previousLevelSymbol 0-8)
-    uint16_t *run_books;     // 6 x 512: a row per distinct run codebook of Table 10
-    uint16_t *level_books;   // 6 x 512: a row per distinct level codebook of Table 11
+    uint16_t *run_books;     // 6 x 512 packed prefix entries: a row per distinct run codebook (Table 10)
+    uint16_t *level_books;   // 6 x 512: a row per distinct level codebook (Table 11)
     float *basis;            // T[x][u] at 8x + u, as the crate computes it
 };
 

@@ -325,8 +325,6 @@ Context::~Context() {
         if (r.graph) cudaGraphExecDestroy(r.graph);
     }
     retired.clear();
-    if (tables.run_decode) cudaFree(tables.run_decode);
-    if (tables.level_decode) cudaFree(tables.level_decode);
     if (tables.run_books) cudaFree(tables.run_books);
     if (tables.level_books) cudaFree(tables.level_books);
     if (tables.basis) cudaFree(tables.basis);
@@ -696,9 +694,6 @@ static int fail(const Status &s) {
 static int fail_or_ok(const Status &s) { return s ? fail(s) : PRORES_OK; }
 
 static Status make_tables(Context &c) {
-    std::vector<uint16_t> run(kRunTableWords), level(kLevelTableWords);
-    build_decode_table(run_book, 16, run.data());
-    build_decode_table(level_book, 9, level.data());
     std::vector<uint16_t> run6(kBookTableWords), level6(kBookTableWords);
     build_book_tables(run6.data(), level6.data());
     PR_CUDA(cudaMalloc(&c.tables.run_books, run6.size() * 2), "cudaMalloc");
@@ -707,11 +702,7 @@ static Status make_tables(Context &c) {
     PR_CUDA(cudaMemcpy(c.tables.level_books, level6.data(), level6.size() * 2, cudaMemcpyHostToDevice), "upload");
     float basis[64];
     dct_basis(basis);
-    PR_CUDA(cudaMalloc(&c.tables.run_decode, run.size() * 2), "cudaMalloc");
-    PR_CUDA(cudaMalloc(&c.tables.level_decode, level.size() * 2), "cudaMalloc");
     PR_CUDA(cudaMalloc(&c.tables.basis, sizeof basis), "cudaMalloc");
-    PR_CUDA(cudaMemcpy(c.tables.run_decode, run.data(), run.size() * 2, cudaMemcpyHostToDevice), "upload");
-    PR_CUDA(cudaMemcpy(c.tables.level_decode, level.data(), level.size() * 2, cudaMemcpyHostToDevice), "upload");
     PR_CUDA(cudaMemcpy(c.tables.basis, basis, sizeof basis, cudaMemcpyHostToDevice), "upload");
     return Status();
 }

@@ -119,8 +119,8 @@ struct Tuning {
     int entropy_components_per_lane = 1;
     int staging_depth = 4;
     int decode_fused = 1;               // one kernel for the per-slice decode (else entropy, then IDCT)
-    int decode_slot_positions = 16384;  // coefficient positions a CTA of the fused decode holds
-    int decode_slot_bytes = 2;          // bytes a coefficient takes there (1: int8, 2: int16)
+    int decode_slot_positions = 65536;  // coefficient positions a CTA of the fused decode holds
+    int decode_slot_bytes = 1;          // bytes a coefficient takes there (1: int8, 2: int16)
 };
 
 struct Context {
