@@ -801,17 +801,30 @@ __device__ __forceinline__ uint64_t mbs_from(const EncPicDesc &pd, const EncSlic
     return (uint64_t)pd.width_in_mb * pd.height_in_mb - ((uint64_t)sd.mb_y * pd.width_in_mb + sd.mb_x);
 }
 
+// The probe step that costed quantiser qi for this picture, or -1. The crate
+// reuses only the probe at uniform - 1 (src/encode.rs:743-749) and costs
+// the later window levels afresh; a size is a function of the slice and
+// the quantiser alone, so reusing any probe at a window's quantiser gives
+// the same sizes and changes no choice.
+__device__ __forceinline__ int probe_step_for(const EncPicState &st, int32_t qi) {
+#pragma unroll
+    for (int k = 0; k < kProbeSteps; k++)
+        if (qi >= 1 && st.step_qi[k] == (uint32_t)qi) return k;
+    return -1;
+}
+
 // Component sizes at window level j (quantiser uniform - 1 - j) of slice s:
-// from the failed probe at uniform - 1 when there is one, else the window.
+// from a probe at that quantiser when there is one, else the window.
 __device__ __forceinline__ const uint32_t *level_comp(const EncodeLaunch &e, const EncPicState &st, uint32_t j,
                                                       uint32_t s) {
-    if (j == 0 && st.lo_probe >= 0) return e.probe_comp + ((uint64_t)st.lo_probe * e.n_slices + s) * 3u;
+    const int step = probe_step_for(st, st.uniform - 1 - (int32_t)j);
+    if (step >= 0) return e.probe_comp + ((uint64_t)step * e.n_slices + s) * 3u;
     return e.win_comp + ((uint64_t)j * e.n_slices + s) * 3u;
 }
 
 // The slices whose window level is costed, as a list: level 0 takes every
-// slice of a picture that has finer quantisers to share out (unless the
-// failed probe at uniform - 1 sized them already); a later level the slices
+// slice of a picture that has finer quantisers to share out; a later level
+// the slices (at no level that a probe sized already)
 // whose size at the level before fits and is within the most their share
 // can come to (the crate's prefetch rule, src/encode.rs:741-767). The list
 // order is the atomics' and steers nothing but speed.
@@ -823,7 +836,7 @@ __global__ void __launch_bounds__(kCostThreads) k_window_select(EncodeLaunch e, 
         const EncSliceDesc sd = e.slices[s];
         const EncPicState st = e.state[sd.pic];
         const int32_t qi = st.uniform - 1 - level;
-        if (st.fits_at_all && st.uniform > 1 && qi >= 1 && !(level == 0 && st.lo_probe >= 0)) {
+        if (st.fits_at_all && st.uniform > 1 && qi >= 1 && probe_step_for(st, qi) < 0) {
             take = true;
             if (level > 0) {
                 const EncPicDesc &pd = e.pics[sd.pic];
@@ -961,6 +974,7 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
     const uint64_t total = block_sum_u64(sum, sh);
     if (threadIdx.x == 0) {
         EncPicState st = st0;
+        st.step_qi[step] = (uint8_t)st.probe_qi;
         const bool ok = all_fit && total <= st.budget;
         if (step == 0) {
             // totals(224): if even the coarsest quantiser does not fit, it is

@@ -66,7 +66,7 @@ struct EncPicState {
     int32_t lo_probe;    // the failed probe step at lo - 1, or -1
     int32_t fits_at_all;
     int32_t uniform;
-    int32_t pad;
+    uint8_t step_qi[12];  // the quantiser each probe step costed (0: none)
 };
 
 // A window entry that was not costed (the share-out costs it if needed).
