@@ -336,6 +336,20 @@ def run_config(name, batch, stream, steps, warmup, check, local):
             out["mismatches"] = bad
     enc.close()
     dec.close()
+    # Where the time goes: one profiled launch of each direction.
+    os.environ["PRORES_PROFILE_KERNELS"] = "1"
+    penc = P.EncodeJob(frames, configs, device=local)
+    pdec = P.DecodeJob(packets, device=local)
+    os.environ.pop("PRORES_PROFILE_KERNELS")
+    for key, job in (("encode_kernels_ms", penc), ("decode_kernels_ms", pdec)):
+        job.launch(stream)
+        stream.synchronize()
+        ms = {}
+        for kname, t in job.kernel_times():
+            if kname.startswith("k_"):
+                ms[kname] = round(ms.get(kname, 0.0) + t, 4)
+        out[key] = dict(sorted(ms.items(), key=lambda x: -x[1]))
+        job.close()
     return name, out
 
 
@@ -611,15 +625,21 @@ def run_serving(args, device):
            "host_buffers": "requests (packets, frames) in page-locked receive buffers; decoded planes into "
                            "pooled page-locked buffers"}
     window = 10.0
-    for name, workers, max_batch, seconds, rate in [
-            ("batched", 4, 16, args.serve_seconds, args.serve_rate),
-            ("batched_half_load", 4, 16, max(1.0, min(20.0, args.serve_seconds / 2)), args.serve_rate / 2),
-            ("plain", 1, 1, max(1.0, min(10.0, args.serve_seconds / 6)), args.serve_rate)]:
+    # (name, workers, batch cap, seconds, offered rate, warm-up rate): a batched
+    # server warms up at the offered rate, so that its workspaces and output
+    # pools have grown to the batches that rate makes before anything is
+    # measured (as a server in service would have); the plain form, which
+    # cannot keep up with that rate, at a rate it can.
+    for name, workers, max_batch, seconds, rate, warm in [
+            ("batched", 4, 16, args.serve_seconds, args.serve_rate, args.serve_rate),
+            ("batched_half_load", 4, 16, max(1.0, min(20.0, args.serve_seconds / 2)), args.serve_rate / 2,
+             args.serve_rate),
+            ("plain", 1, 1, max(1.0, min(10.0, args.serve_seconds / 6)), args.serve_rate, 200.0)]:
         # One backend (and its pool of page-locked output buffers) for the
         # warm-up and the measured run.
         backend = S.GpuBackend(device)
         srv = S.Server(backend, memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
-        S.poisson_run(srv, maker(1), rate=200.0, seconds=0.3)  # workspaces allocated, not measured
+        S.poisson_run(srv, maker(1), rate=warm, seconds=2.0 if warm > 200.0 else 0.3)  # not measured
         srv.close()
         srv = S.Server(backend, memory_budget=8 << 30, max_batch=max_batch, workers=workers, device=device)
         st = S.poisson_run(srv, maker(2), rate=rate, seconds=seconds, window=window)

@@ -227,15 +227,40 @@ struct Window {
     }
 };
 
+// The codeword of codebook `cb` at the top of `t` (32 bits, all data), as
+// read_sym's general path reads it, when it is no longer than 32 bits and
+// its symbol is in range; false otherwise (read_sym then reads it, and
+// names any failure).
+__device__ __forceinline__ bool window_code(uint32_t t, Codebook cb, uint32_t &sym, uint32_t &len) {
+    const uint32_t lz = __clz(t);
+    if (!cb.eg && lz <= cb.q) {
+        len = lz + 1u + cb.r;
+        sym = (lz << cb.r) | (cb.r ? (t << (lz + 1u)) >> (32u - cb.r) : 0u);
+        return true;
+    }
+    const uint32_t qe = cb.eg ? lz : lz - (cb.q + 1u);
+    const uint32_t ke = cb.eg ? cb.r : cb.e;
+    const uint32_t need = qe + ke + 1u;
+    if (lz + need > 32u) return false;
+    len = lz + need;
+    const uint64_t n = (uint64_t)((t << lz) >> (32u - need)) - (1ull << ke) +
+                       (cb.eg ? 0ull : (uint64_t)(cb.q + 1u) << cb.r);
+    if (n > kMaxSymbol) return false;
+    sym = (uint32_t)n;
+    return true;
+}
+
 // scanned_coefficients() of one component (src/decode.rs:484-540): every
 // coefficient the codes give, in scanned-index order, handed to `out.put`
 // (position, value); the positions not handed over are zero. `run_tab` and
 // `level_tab` are the packed prefix tables of build_book_tables (a row per
-// distinct codebook): while 32 or more bits remain, a run, level and sign
-// whose codewords are both in them are read from the window in one go (all
-// the bits they take are data, and the tables give the symbols the general
-// reader would); anything else, and the end of the data, goes through the
-// general reader, which also names every failure as the crate does.
+// distinct codebook). While 32 or more bits remain, codes are read from the
+// window: a run, level and sign whose codewords are both in the tables in
+// one go, any other codeword of up to 32 bits by window_code, a symbol at a
+// time (all the bits they take are data, so they come out as the general
+// reader would read them). A longer codeword and the last bits of the data
+// go through the general reader, which also names every failure as the
+// crate does.
 template <class Out>
 __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
@@ -257,31 +282,81 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
     }
     const uint32_t total = n_blocks * 64;
     uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
+    bool level_next = false;  // a run was read; its level and sign come next
     for (;;) {
         if (b.remaining() >= 32) {
             Window win;
             win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
             uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
             while (win.left >= 32u) {
-                const uint32_t t = win.top();
-                const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
-                if (!e1) break;
-                const uint32_t l1 = e1 & 15u, t2 = t << l1;
-                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
-                if (!e2) break;
-                const uint32_t l2 = e2 & 15u;
-                prev_run = (e1 >> 4) & 63u;
-                prev_level = (e2 >> 4) & 63u;
-                n += prev_run;
-                if (n >= total) return DE_RUN_PAST_END;
-                const int32_t level = (int32_t)prev_level + 1;
-                out.put(n, (t2 << l2) >> 31 ? -level : level);
+                uint32_t t = win.top(), l;
+                if (!level_next) {
+                    const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
+                    if (e1) {
+                        const uint32_t l1 = e1 & 15u, t2 = t << l1;
+                        const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
+                        if (e2) {
+                            // Run, level and sign in one go.
+                            const uint32_t l2 = e2 & 15u;
+                            prev_run = (e1 >> 4) & 63u;
+                            prev_level = (e2 >> 4) & 63u;
+                            n += prev_run;
+                            if (n >= total) return DE_RUN_PAST_END;
+                            const int32_t level = (int32_t)prev_level + 1;
+                            out.put(n, (t2 << l2) >> 31 ? -level : level);
+                            n += 1;
+                            rrow = (e1 >> 10) * kDecodeEntries;
+                            lrow = (e2 >> 10) * kDecodeEntries;
+                            win.consume(l1 + l2 + 1u);
+                            continue;
+                        }
+                        prev_run = (e1 >> 4) & 63u;
+                        l = l1;
+                    } else if (!window_code(t, run_book(prev_run), prev_run, l)) {
+                        break;
+                    }
+                    n += prev_run;
+                    if (n >= total) return DE_RUN_PAST_END;
+                    win.consume(l);
+                    level_next = true;
+                    if (win.left < 32u) break;
+                    t = win.top();
+                }
+                uint32_t lvl;
+                const uint32_t e2 = level_tab[lrow + (t >> (32 - kDecodeBits))];
+                if (e2) {
+                    lvl = (e2 >> 4) & 63u;
+                    l = e2 & 15u;
+                } else if (!window_code(t, level_book(prev_level), lvl, l)) {
+                    break;
+                }
+                win.consume(l);
+                prev_level = lvl;
+                if (win.left == 0) return DE_PAST_END;
+                const bool neg = win.top() >> 31;
+                win.consume(1u);
+                const int32_t level = (int32_t)lvl + 1;
+                out.put(n, neg ? -level : level);
                 n += 1;
-                rrow = (e1 >> 10) * kDecodeEntries;
-                lrow = (e2 >> 10) * kDecodeEntries;
-                win.consume(l1 + l2 + 1u);
+                level_next = false;
+                rrow = run_book_row(prev_run) * kDecodeEntries;
+                lrow = level_book_row(prev_level) * kDecodeEntries;
             }
             b.pos = b.end - win.left;
+        }
+        if (level_next) {
+            // A level and sign the window could not read.
+            uint32_t lvl;
+            if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return err;
+            prev_level = lvl;
+            if (b.remaining() < 1) return DE_PAST_END;
+            const bool neg = b.peek() >> 63;
+            b.pos += 1;
+            const int32_t level = (int32_t)lvl + 1;
+            out.put(n, neg ? -level : level);
+            n += 1;
+            level_next = false;
+            continue;
         }
         if (b.remaining() <= 31 && b.peek() == 0) break;  // endOfData()
         uint32_t run, lvl;
