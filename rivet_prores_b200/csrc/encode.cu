@@ -912,6 +912,56 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
     }
 }
 
+// The levels past the window, costed ahead of the share-out, a warp per
+// slice, every slice at once: a slice whose last window level fits and is
+// within the most its share can come to (the window's prefetch rule) goes
+// on to the next finer quantiser, and so on while the size it just found
+// fits and stays within that most, for up to kDeepLevels levels. A slice's
+// ladder depends on nothing but its own sizes and its picture's slack, so
+// the slices need not wait for one another; the share-out then reads these
+// sizes instead of costing them one slice after another (which it still
+// does for a level past the ladder).
+__global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
+    __shared__ LenTables t;
+    t.fill();
+    __syncthreads();
+    const uint32_t s = blockIdx.x * (kCostThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= e.n_slices) return;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicState st = e.state[sd.pic];
+    uint32_t count = 0;
+    if (st.fits_at_all && st.uniform - kWindow > 1) {
+        const EncPicDesc &pd = e.pics[sd.pic];
+        const EncFrameDesc &fd = e.frames[pd.frame];
+        const uint32_t hb = pd.header_bytes, alpha = e.alpha_bytes[s];
+        const uint32_t *u = e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u;
+        const uint32_t uc[3] = {u[0], u[1], u[2]};
+        bool f0;
+        const uint64_t used = slice_total(hb, uc, alpha, f0);
+        const uint64_t most = used + (st.budget - st.hi_total) * sd.mbs / mbs_from(pd, sd);
+        const uint32_t *c = level_comp(e, st, kWindow - 1, s);
+        bool fits = false;
+        uint64_t n = ~0ull;
+        if (c[0] != kNotCosted) {
+            const uint32_t cc[3] = {c[0], c[1], c[2]};
+            n = slice_total(hb, cc, alpha, fits);
+        }
+        for (uint32_t j = 0; fits && n <= most && j < (uint32_t)kDeepLevels; j++) {
+            const int32_t qi = st.uniform - 1 - kWindow - (int32_t)j;
+            if (qi < 1) break;
+            uint32_t c3[3];
+            for (uint32_t comp = 0; comp < 3; comp++) c3[comp] = warp_component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+            n = slice_total(hb, c3, alpha, fits);
+            if (lane == 0)
+                e.deep[(uint64_t)s * kDeepLevels + j] =
+                    make_uint2(min(c3[0], 65535u) | (min(c3[1], 65535u) << 16), min(c3[2], 65535u) | ((fits ? 1u : 0u) << 16));
+            count = j + 1;
+        }
+    }
+    if (lane == 0) e.deep_count[s] = count;
+}
+
 constexpr int kRcThreads = 256;
 
 __device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, uint64_t *sh) {
@@ -1014,10 +1064,11 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_step(EncodeLaunch e, int step
 //   k_share_prep   every slice in parallel: its base and, for each window
 //                  level, the threshold on D and the size over the base;
 //   k_shareout     one warp per picture, the only serial part: D against
-//                  the thresholds, 32 slices at a time by ballot, each
-//                  stepping slice settled by its own lane; the warp costs a
-//                  deeper quantiser together when a slice gets past the
-//                  window;
+//                  the thresholds (the window's, then each slice's deep
+//                  ladder from k_cost_deep), 32 slices at a time by ballot,
+//                  each stepping slice settled by its own lane; the warp
+//                  costs a deeper quantiser together when a slice gets past
+//                  all of them;
 //   k_share_final  every slice in parallel: its quantiser and sizes.
 constexpr uint32_t kDeepFlag = 0x80000000u;  // share_steps: sizes are in final_comp already
 
@@ -1037,6 +1088,10 @@ __global__ void k_share_prep(EncodeLaunch e) {
         const uint64_t rem = mbs_from(pd, sd);
         const uint32_t shift = 31u - __clz(sd.mbs);
         pr.base = (uint32_t)base;
+        pr.hba = hb + alpha;
+        pr.rem = (uint32_t)rem;
+        pr.shift = shift;
+        pr.deep_count = e.deep_count[s];
 #pragma unroll
         for (int j = 0; j < kWindow; j++) {
             pr.thr[j] = ~0ull;
@@ -1054,25 +1109,56 @@ __global__ void k_share_prep(EncodeLaunch e) {
     e.share_prep[s] = pr;
 }
 
+// A level past the window from a slice's deep ladder: its size, and whether
+// it fits.
+__device__ __forceinline__ uint64_t deep_size(const SharePrep &p, uint2 v, bool &fits) {
+    fits = (v.y >> 16) != 0;
+    return (uint64_t)p.hba + (v.x & 0xFFFFu) + (v.x >> 16) + (v.y & 0xFFFFu);
+}
+
 // Steps a slice takes at D through its known levels (the walk of
-// src/encode.rs:776-788 while the sizes are known), and whether it then
-// needs a level nobody costed (`deep`).
-__device__ __forceinline__ uint32_t steps_at(const SharePrep &p, uint64_t D, int32_t uniform, bool &deep) {
-    deep = false;
+// src/encode.rs:776-788 while the sizes are known: the window's, then its
+// deep ladder `deep`), and whether it then needs a level nobody costed
+// (`deep_needed`).
+__device__ __forceinline__ uint32_t steps_at(const SharePrep &p, const uint2 *deep, uint64_t D, int32_t uniform,
+                                             bool &deep_needed) {
+    deep_needed = false;
     uint32_t k = 0;
 #pragma unroll
     for (int j = 0; j < kWindow; j++) {
         // k == j steps so far: the quantiser is uniform - j.
         if (uniform - j <= 1) return k;
         if (!((p.known >> j) & 1u)) {
-            deep = true;
+            deep_needed = true;
             return k;
         }
         if (D < p.thr[j]) return k;
         k++;
     }
-    deep = uniform - kWindow > 1;
+    for (uint32_t j = 0; j < p.deep_count; j++) {
+        if (uniform - (int32_t)k <= 1) return k;
+        bool fits;
+        const uint64_t n = deep_size(p, deep[j], fits);
+        if (!fits) return k;
+        const uint64_t thr = n <= p.base ? 0ull : (((n - p.base) * p.rem) + (1u << p.shift) - 1u) >> p.shift;
+        if (D < thr) return k;
+        k++;
+    }
+    deep_needed = uniform - (int32_t)k > 1;
     return k;
+}
+
+// The size over the base after `ks` steps (ks >= 1).
+__device__ __forceinline__ int64_t delta_at(const SharePrep &p, const uint2 *deep, uint32_t ks) {
+    if (ks <= (uint32_t)kWindow) {
+        int32_t d = p.delta[0];
+#pragma unroll
+        for (int j = 1; j < kWindow; j++)
+            if ((uint32_t)j + 1u == ks) d = p.delta[j];
+        return d;
+    }
+    bool fits;
+    return (int64_t)deep_size(p, deep[ks - 1u - kWindow], fits) - (int64_t)p.base;
 }
 
 constexpr int kShareWarps = 1;
@@ -1104,6 +1190,7 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
         const SharePrep mine = next;
         const uint32_t k = k0 + lane;
         const bool live = k < pd.n_slices;
+        const uint2 *my_deep = e.deep + (uint64_t)(pd.slice_base + (live ? k : 0u)) * kDeepLevels;
         // The next chunk's thresholds, fetched while this chunk is walked.
         if (k + 32 < pd.n_slices) next = e.share_prep[pd.slice_base + k + 32];
         uint32_t my_steps = 0;
@@ -1123,13 +1210,10 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
             uint32_t first_deep = 32;
             for (int round = 0; round < 34; round++) {
                 bool deep = false;
-                ks = live && (uint32_t)lane >= done ? steps_at(mine, myD, st.uniform, deep) : 0u;
+                ks = live && (uint32_t)lane >= done ? steps_at(mine, my_deep, myD, st.uniform, deep) : 0u;
                 const uint32_t deep_mask = __ballot_sync(0xffffffffu, live && (uint32_t)lane >= done && deep);
                 const uint32_t fd_lane = deep_mask ? (uint32_t)__ffs(deep_mask) - 1u : 32u;
-                int64_t mine_dl = 0;
-#pragma unroll
-                for (int j = 0; j < kWindow; j++)
-                    if ((uint32_t)j + 1u == ks) mine_dl = mine.delta[j];
+                const int64_t mine_dl = ks ? delta_at(mine, my_deep, ks) : 0;
                 dl = (uint32_t)lane < fd_lane ? mine_dl : 0;
                 // Inclusive sum of dl over the lanes.
                 int64_t incl = dl;
@@ -1160,10 +1244,8 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
             D = (uint64_t)((int64_t)D - settled);
             const uint32_t f = first_deep;
             const uint32_t fk = __shfl_sync(0xffffffffu, ks, f);
-            int64_t delta = fk ? (int64_t)__shfl_sync(0xffffffffu, mine.delta[0], f) : 0;
-#pragma unroll
-            for (int j = 1; j < kWindow; j++)
-                if ((uint32_t)j == fk - 1) delta = __shfl_sync(0xffffffffu, mine.delta[j], f);
+            const int64_t my_delta = ks ? delta_at(mine, my_deep, ks) : 0;
+            int64_t delta = __shfl_sync(0xffffffffu, my_delta, f);
             uint32_t steps = fk;
             {
                 const uint32_t s = pd.slice_base + k0 + f;
@@ -1231,6 +1313,15 @@ __global__ void k_share_final(EncodeLaunch e) {
     const uint32_t n = steps & ~kDeepFlag;
     e.final_qi[s] = (uint32_t)st.uniform - n;
     if (steps & kDeepFlag) return;  // written by the walk
+    if (n > (uint32_t)kWindow) {
+        // From the slice's deep ladder (a level the slice fits at, so no
+        // size there is saturated).
+        const uint2 v = e.deep[(uint64_t)s * kDeepLevels + (n - 1u - kWindow)];
+        e.final_comp[3ull * s] = v.x & 0xFFFFu;
+        e.final_comp[3ull * s + 1] = v.x >> 16;
+        e.final_comp[3ull * s + 2] = v.y & 0xFFFFu;
+        return;
+    }
     const uint32_t *c = n == 0 ? e.probe_comp + ((uint64_t)st.hi_probe * e.n_slices + s) * 3u
                                : level_comp(e, st, n - 1u, s);
     e.final_comp[3ull * s] = c[0];
@@ -1560,6 +1651,12 @@ cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s)
             e, level);
     else
         k_cost_window<true><<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, level);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cost_deep(const EncodeLaunch &e, cudaStream_t s) {
+    if (!e.n_slices) return cudaSuccess;
+    k_cost_deep<<<(e.n_slices + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e);
     return cudaGetLastError();
 }
 

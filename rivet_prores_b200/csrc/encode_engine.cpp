@@ -305,6 +305,11 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     o += sizeof(SharePrep) * ns;
     e.share_steps = reinterpret_cast<uint32_t *>(base + o);
     o += 4 * ns;
+    e.deep_count = reinterpret_cast<uint32_t *>(base + o);
+    o += 4 * ns;
+    o = (o + 15) & ~(size_t)15;
+    e.deep = reinterpret_cast<uint2 *>(base + o);
+    o += sizeof(uint2) * kDeepLevels * ns;
     e.win_list = reinterpret_cast<uint32_t *>(base + o);
     o += 4 * ns;
     e.win_count = reinterpret_cast<uint32_t *>(base + o);
@@ -324,7 +329,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
 static size_t cost_bytes(const EncodePlan &plan) {
     const size_t ns = plan.n_slices + 1;
     return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 4 * ns +
-           4 * kWindow + 256;
+           4 * ns + sizeof(uint2) * kDeepLevels * ns + 4 * kWindow + 256;
 }
 
 static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s,
@@ -429,6 +434,8 @@ Status enqueue_encode(Context &ctx, Workspace &ws, EncodePlan &plan, cudaStream_
         PR_CUDA(launch_cost_window(e, level, s), "k_cost_window");
         if ((st = record_kernel(kt, "k_cost_window", s))) return st;
     }
+    PR_CUDA(launch_cost_deep(e, s), "k_cost_deep");
+    if ((st = record_kernel(kt, "k_cost_deep", s))) return st;
     PR_CUDA(launch_shareout(e, s), "k_shareout");
     if ((st = record_kernel(kt, "k_shareout", s))) return st;
     return enqueue_tail(ctx, ws, plan, s, kt);

@@ -14,6 +14,10 @@ constexpr int kProbeSteps = 9;
 // the next ones for the slices that could reach them); the share-out costs
 // anything else it needs itself.
 constexpr int kWindow = 4;
+// Finer quantisers past the window costed ahead of the share-out for a
+// slice that could reach them (the same prefetch rule, level after level):
+// at most this many per slice; the share-out costs any further one itself.
+constexpr int kDeepLevels = 64;
 // Bytes per frame-header template: 8 + a frame_header() of at most 148.
 constexpr uint32_t kHeaderSlot = 160;
 
@@ -80,6 +84,10 @@ struct SharePrep {
     int32_t delta[kWindow];
     uint32_t base;
     uint32_t known;
+    // For the levels past the window (deep_count of them, in `deep`): the
+    // slice header and alpha bytes, the macroblocks from the slice to the
+    // end of the picture, and log2 of the slice's macroblocks.
+    uint32_t hba, rem, shift, deep_count;
 };
 
 // Per quantiser set and quantization_index, kQuantStride floats:
@@ -112,6 +120,9 @@ struct EncodeLaunch {
     uint64_t *slice_off;   // [slice] byte offset of the slice in its frame
     SharePrep *share_prep; // [slice]
     uint32_t *share_steps; // [slice] finer steps taken (top bit: sizes already in final_comp)
+    uint2 *deep;           // [slice][kDeepLevels] component bytes past the window: x = Y' | Cb << 16,
+                           //   y = Cr | fits << 16 (sizes saturate at 65535, which never fits)
+    uint32_t *deep_count;  // [slice] levels in deep
     uint32_t *out;         // output buffer (zeroed before packing), big-endian bit order
     const uint8_t *headers;  // frame header templates
     uint32_t *frame_status;  // per frame: 0, or 1 when the frame outgrew its region
@@ -128,6 +139,7 @@ cudaError_t launch_rc_init(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s);
 cudaError_t launch_rc_step(const EncodeLaunch &e, int step, cudaStream_t s);
 cudaError_t launch_cost_window(const EncodeLaunch &e, int level, cudaStream_t s);
+cudaError_t launch_cost_deep(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s);
 cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s);
