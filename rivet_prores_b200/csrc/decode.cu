@@ -282,96 +282,102 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
     }
     const uint32_t total = n_blocks * 64;
     uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
-    bool level_next = false;  // a run was read; its level and sign come next
+    // One run, level and sign an iteration: from the window while it holds
+    // the read position and 32 or more bits remain, else by the general
+    // reader (which then hands the position back to a fresh window). A lane
+    // that takes the general reader leaves the others only for that one
+    // iteration.
+    Window win;
+    bool in_win = b.remaining() >= 32;
+    if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
+    uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
     for (;;) {
-        if (b.remaining() >= 32) {
-            Window win;
-            win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
-            uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
-            while (win.left >= 32u) {
-                uint32_t t = win.top(), l;
-                if (!level_next) {
-                    const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
-                    if (e1) {
-                        const uint32_t l1 = e1 & 15u, t2 = t << l1;
-                        const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
-                        if (e2) {
-                            // Run, level and sign in one go.
-                            const uint32_t l2 = e2 & 15u;
-                            prev_run = (e1 >> 4) & 63u;
-                            prev_level = (e2 >> 4) & 63u;
-                            n += prev_run;
-                            if (n >= total) return DE_RUN_PAST_END;
-                            const int32_t level = (int32_t)prev_level + 1;
-                            out.put(n, (t2 << l2) >> 31 ? -level : level);
-                            n += 1;
-                            rrow = (e1 >> 10) * kDecodeEntries;
-                            lrow = (e2 >> 10) * kDecodeEntries;
-                            win.consume(l1 + l2 + 1u);
-                            continue;
-                        }
-                        prev_run = (e1 >> 4) & 63u;
-                        l = l1;
-                    } else if (!window_code(t, run_book(prev_run), prev_run, l)) {
-                        break;
-                    }
-                    n += prev_run;
-                    if (n >= total) return DE_RUN_PAST_END;
-                    win.consume(l);
-                    level_next = true;
-                    if (win.left < 32u) break;
-                    t = win.top();
-                }
-                uint32_t lvl;
-                const uint32_t e2 = level_tab[lrow + (t >> (32 - kDecodeBits))];
+        bool level_next = false;  // the run is read; its level and sign are the general reader's
+        if (in_win && win.left >= 32u) {
+            const uint32_t t = win.top();
+            const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
+            uint32_t run = 0, l = 0;
+            bool got = true;
+            if (e1) {
+                l = e1 & 15u;
+                run = (e1 >> 4) & 63u;
+                const uint32_t t2 = t << l;
+                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
                 if (e2) {
-                    lvl = (e2 >> 4) & 63u;
-                    l = e2 & 15u;
-                } else if (!window_code(t, level_book(prev_level), lvl, l)) {
-                    break;
+                    // Run, level and sign in one go.
+                    const uint32_t l2 = e2 & 15u;
+                    prev_run = run;
+                    prev_level = (e2 >> 4) & 63u;
+                    n += run;
+                    if (n >= total) return DE_RUN_PAST_END;
+                    const int32_t level = (int32_t)prev_level + 1;
+                    out.put(n, (t2 << l2) >> 31 ? -level : level);
+                    n += 1;
+                    rrow = (e1 >> 10) * kDecodeEntries;
+                    lrow = (e2 >> 10) * kDecodeEntries;
+                    win.consume(l + l2 + 1u);
+                    continue;
                 }
-                win.consume(l);
-                prev_level = lvl;
-                if (win.left == 0) return DE_PAST_END;
-                const bool neg = win.top() >> 31;
-                win.consume(1u);
-                const int32_t level = (int32_t)lvl + 1;
-                out.put(n, neg ? -level : level);
-                n += 1;
-                level_next = false;
-                rrow = run_book_row(prev_run) * kDecodeEntries;
-                lrow = level_book_row(prev_level) * kDecodeEntries;
+            } else {
+                got = window_code(t, run_book(prev_run), run, l);
             }
-            b.pos = b.end - win.left;
+            if (got) {
+                prev_run = run;
+                n += run;
+                if (n >= total) return DE_RUN_PAST_END;
+                win.consume(l);
+                uint32_t lvl = 0;
+                got = false;
+                if (win.left >= 32u) {
+                    const uint32_t u = win.top();
+                    const uint32_t e2 = level_tab[lrow + (u >> (32 - kDecodeBits))];
+                    if (e2) {
+                        lvl = (e2 >> 4) & 63u;
+                        l = e2 & 15u;
+                        got = true;
+                    } else {
+                        got = window_code(u, level_book(prev_level), lvl, l);
+                    }
+                }
+                if (got) {
+                    win.consume(l);
+                    prev_level = lvl;
+                    if (win.left == 0) return DE_PAST_END;
+                    const bool neg = win.top() >> 31;
+                    win.consume(1u);
+                    const int32_t level = (int32_t)lvl + 1;
+                    out.put(n, neg ? -level : level);
+                    n += 1;
+                    rrow = run_book_row(prev_run) * kDecodeEntries;
+                    lrow = level_book_row(prev_level) * kDecodeEntries;
+                    continue;
+                }
+                level_next = true;
+            }
         }
-        if (level_next) {
-            // A level and sign the window could not read.
-            uint32_t lvl;
-            if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return err;
-            prev_level = lvl;
-            if (b.remaining() < 1) return DE_PAST_END;
-            const bool neg = b.peek() >> 63;
-            b.pos += 1;
-            const int32_t level = (int32_t)lvl + 1;
-            out.put(n, neg ? -level : level);
-            n += 1;
-            level_next = false;
-            continue;
+        // The general reader, from the window's position.
+        if (in_win) b.pos = b.end - win.left;
+        if (!level_next) {
+            if (b.remaining() <= 31 && b.peek() == 0) break;  // endOfData()
+            uint32_t run;
+            if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return err;
+            prev_run = run;
+            n += run;
+            if (n >= total) return DE_RUN_PAST_END;
         }
-        if (b.remaining() <= 31 && b.peek() == 0) break;  // endOfData()
-        uint32_t run, lvl;
-        if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return err;
-        prev_run = run;
-        n += run;
-        if (n >= total) return DE_RUN_PAST_END;
+        uint32_t lvl;
         if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return err;
         prev_level = lvl;
         if (b.remaining() < 1) return DE_PAST_END;
-        bool neg = b.peek() >> 63;
+        const bool neg = b.peek() >> 63;
         b.pos += 1;
-        int32_t level = (int32_t)lvl + 1;
+        const int32_t level = (int32_t)lvl + 1;
         out.put(n, neg ? -level : level);
         n += 1;
+        rrow = run_book_row(prev_run) * kDecodeEntries;
+        lrow = level_book_row(prev_level) * kDecodeEntries;
+        in_win = b.remaining() >= 32;
+        if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
     }
     return DE_OK;
 }
