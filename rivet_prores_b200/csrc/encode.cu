@@ -914,13 +914,24 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
 
 // The levels past the window, costed ahead of the share-out, a warp per
 // slice, every slice at once: a slice whose last window level fits and is
-// within the most its share can come to (the window's prefetch rule) goes
-// on to the next finer quantiser, and so on while the size it just found
-// fits and stays within that most, for up to kDeepLevels levels. A slice's
-// ladder depends on nothing but its own sizes and its picture's slack, so
-// the slices need not wait for one another; the share-out then reads these
-// sizes instead of costing them one slice after another (which it still
-// does for a level past the ladder).
+// within its likely allowance goes on to the next finer quantiser, and so
+// on while the size it just found fits and stays within that allowance,
+// for up to kDeepLevels levels. A slice's ladder depends on nothing but its
+// own sizes and its picture's slack, so the slices need not wait for one
+// another; the share-out then reads these sizes instead of costing them one
+// slice after another (which it still does for a level past the ladder).
+//
+// The likely allowance is the slice's share of the picture's slack in
+// proportion to its macroblocks, plus a quarter, plus one step (its size
+// change at the first finer quantiser), and never above the most its share
+// can come to (the crate's prefetch rule: the whole slack from the slice on,
+// if no slice before it took any). The share-out's allowance for a slice is
+// what the slices before it left, which stays near the proportional share
+// but for the last few slices of a picture; the most is far above it there
+// (the last slice's is the whole slack), and a ladder to the most costed
+// several quantisers of every slice of a picture's tail for nothing. What
+// the ladder leaves out only moves work to the share-out, never changes a
+// size.
 __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
     __shared__ LenTables t;
     t.fill();
@@ -939,7 +950,18 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
         const uint32_t uc[3] = {u[0], u[1], u[2]};
         bool f0;
         const uint64_t used = slice_total(hb, uc, alpha, f0);
-        const uint64_t most = used + (st.budget - st.hi_total) * sd.mbs / mbs_from(pd, sd);
+        const uint64_t slack = st.budget - st.hi_total;
+        const uint64_t most = used + slack * sd.mbs / mbs_from(pd, sd);
+        const uint64_t share = slack * sd.mbs / ((uint64_t)pd.width_in_mb * pd.height_in_mb);
+        const uint32_t *c1 = level_comp(e, st, 0, s);
+        uint64_t step = 0;
+        if (c1[0] != kNotCosted) {
+            const uint32_t cc[3] = {c1[0], c1[1], c1[2]};
+            bool f1;
+            const uint64_t n1 = slice_total(hb, cc, alpha, f1);
+            step = n1 > used ? n1 - used : 0u;
+        }
+        const uint64_t likely = min(most, used + share + share / 4u + step);
         const uint32_t *c = level_comp(e, st, kWindow - 1, s);
         bool fits = false;
         uint64_t n = ~0ull;
@@ -947,7 +969,7 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
             const uint32_t cc[3] = {c[0], c[1], c[2]};
             n = slice_total(hb, cc, alpha, fits);
         }
-        for (uint32_t j = 0; fits && n <= most && j < (uint32_t)kDeepLevels; j++) {
+        for (uint32_t j = 0; fits && n <= likely && j < (uint32_t)kDeepLevels; j++) {
             const int32_t qi = st.uniform - 1 - kWindow - (int32_t)j;
             if (qi < 1) break;
             uint32_t c3[3];
@@ -1118,8 +1140,8 @@ __device__ __forceinline__ uint64_t deep_size(const SharePrep &p, uint2 v, bool 
 
 // Steps a slice takes at D through its known levels (the walk of
 // src/encode.rs:776-788 while the sizes are known: the window's, then its
-// deep ladder `deep`), and whether it then needs a level nobody costed
-// (`deep_needed`).
+// deep ladder, level j at deep[32 j]), and whether it then needs a level
+// nobody costed (`deep_needed`).
 __device__ __forceinline__ uint32_t steps_at(const SharePrep &p, const uint2 *deep, uint64_t D, int32_t uniform,
                                              bool &deep_needed) {
     deep_needed = false;
@@ -1138,7 +1160,7 @@ __device__ __forceinline__ uint32_t steps_at(const SharePrep &p, const uint2 *de
     for (uint32_t j = 0; j < p.deep_count; j++) {
         if (uniform - (int32_t)k <= 1) return k;
         bool fits;
-        const uint64_t n = deep_size(p, deep[j], fits);
+        const uint64_t n = deep_size(p, deep[32u * j], fits);
         if (!fits) return k;
         const uint64_t thr = n <= p.base ? 0ull : (((n - p.base) * p.rem) + (1u << p.shift) - 1u) >> p.shift;
         if (D < thr) return k;
@@ -1158,7 +1180,7 @@ __device__ __forceinline__ int64_t delta_at(const SharePrep &p, const uint2 *dee
         return d;
     }
     bool fits;
-    return (int64_t)deep_size(p, deep[ks - 1u - kWindow], fits) - (int64_t)p.base;
+    return (int64_t)deep_size(p, deep[32u * (ks - 1u - kWindow)], fits) - (int64_t)p.base;
 }
 
 constexpr int kShareWarps = 1;
@@ -1169,6 +1191,10 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     // its chunk maxima): the warp walks it for every quantiser it tries,
     // and from DRAM each of its chunks waited out a full load.
     __shared__ __align__(16) float stage[kShareWarps][kMaxSliceCoefs + kMaxSliceCoefs / 32];
+    // The ladders of the 32 slices a warp settles, level j of lane l at
+    // [32 j + l]: the settling rounds walk them again and again, and from
+    // global memory every level of the walk was a dependent load.
+    __shared__ uint2 ladders[kShareWarps][32 * kDeepLevels];
     t.fill();
     __syncthreads();
     const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
@@ -1190,7 +1216,14 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
         const SharePrep mine = next;
         const uint32_t k = k0 + lane;
         const bool live = k < pd.n_slices;
-        const uint2 *my_deep = e.deep + (uint64_t)(pd.slice_base + (live ? k : 0u)) * kDeepLevels;
+        uint2 *my_deep = ladders[threadIdx.x >> 5] + lane;
+        __syncwarp();  // the last chunk's walks are over
+        if (live) {
+            const uint2 *src = e.deep + (uint64_t)(pd.slice_base + k) * kDeepLevels;
+#pragma unroll 4
+            for (uint32_t j = 0; j < mine.deep_count; j++) my_deep[32u * j] = src[j];
+        }
+        __syncwarp();
         // The next chunk's thresholds, fetched while this chunk is walked.
         if (k + 32 < pd.n_slices) next = e.share_prep[pd.slice_base + k + 32];
         uint32_t my_steps = 0;
