@@ -25,13 +25,26 @@
 
 #include "codec_tables.h"
 #include "device_types.h"
+#include "pair_math.h"
 
 namespace prores {
 
 __constant__ uint8_t c_scan[2][64];
 __constant__ float c_idct_basis[64];  // T[x][u] (dct_basis)
+// The basis as pairs down a column: idct_pair(4 u + j) = (T[2 j][u], T[2 j + 1][u]).
+__constant__ __align__(16) float c_idct_pairs[64];
 
 namespace {
+
+__device__ __forceinline__ uint64_t idct_pair(uint32_t k) { return reinterpret_cast<const uint64_t *>(c_idct_pairs)[k]; }
+
+// floor(v) clamped to [0, max] (max an integer below 2^16), as an integer:
+// clamping before the floor gives the same value as after it for integer
+// bounds, and adding 2^23 rounded down leaves floor(v) in the low bits.
+__device__ __forceinline__ uint32_t floor_clamped(float v, float max) {
+    const float c = fminf(fmaxf(v, 0.0f), max);
+    return __float_as_uint(__fadd_rd(c, 8388608.0f)) & 0xFFFFu;
+}
 
 __device__ __forceinline__ uint64_t bswap64(uint64_t v) {
     uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
@@ -749,12 +762,16 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         }
         held_any[k] = any;
         if (any) {
+            // Outputs x = 2 j, 2 j + 1 a pair, each sum in the same order.
+            uint64_t rr[8];
 #pragma unroll
-            for (int x = 0; x < 8; x++) {
-                float acc = 0.0f;
+            for (int u = 0; u < 8; u++) rr[u] = pair_of(row[u], row[u]);
 #pragma unroll
-                for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, __fmul_rn(row[u], c_idct_basis[8 * x + u]));
-                held[k][x] = acc;
+            for (int j = 0; j < 4; j++) {
+                uint64_t acc = 0;
+#pragma unroll
+                for (int u = 0; u < 8; u++) acc = pair_add(acc, pair_mul(rr[u], idct_pair(4u * u + j)));
+                pair_split(acc, held[k][2 * j], held[k][2 * j + 1]);
             }
         }
     }
@@ -784,11 +801,8 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
     // memory as pairs, [y][column pair][blk] per component.
     const float oscale = fd.out_scale, obias = fd.out_bias, omax = fd.out_max;
     uint32_t *stage = reinterpret_cast<uint32_t *>(smem + 4 * kMaxSliceCoefs + kMaxSliceCoefs / 8);
-    const auto convert = [&](float a) {
-        float v = floorf(__fadd_rn(__fmul_rn(a, oscale), obias));
-        v = v < 0.0f ? 0.0f : (v > omax ? omax : v);
-        return (uint32_t)v;
-    };
+    // floor(v) clamped to [0, max] of the converted value v = a scale + bias.
+    const auto convert = [&](float v) { return floor_clamped(v, omax); };
     for (uint32_t t = tid; t < all_blocks * 4u; t += kIdctThreads) {
         const uint32_t c = t < luma_blocks * 4u ? 0u : (t < (luma_blocks + chroma_blocks) * 4u ? 1u : 2u);
         const uint32_t tc = t - start_of(c) / 16u;  // 4 column tasks a block
@@ -796,23 +810,32 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t blk = tc % nb, j = tc / nb;
         const float *src = tmp + start_of(c) + 2u * j * nb + blk;
         const uint64_t rows = *reinterpret_cast<const uint64_t *>(nz + (start_of(c) / 64u + blk) * 8u);
-        float a0[8], a1[8];
+        // Outputs y = 2 i, 2 i + 1 of each column a pair.
+        uint64_t a0[4], a1[4];
 #pragma unroll
-        for (int y = 0; y < 8; y++) a0[y] = a1[y] = 0.0f;
+        for (int i = 0; i < 4; i++) a0[i] = a1[i] = 0;
 #pragma unroll
         for (int v = 0; v < 8; v++) {
             if (!((rows >> (8 * v)) & 0xffu)) continue;
             const float t0 = src[8u * v * nb], t1 = src[8u * v * nb + nb];
+            const uint64_t d0 = pair_of(t0, t0), d1 = pair_of(t1, t1);
 #pragma unroll
-            for (int y = 0; y < 8; y++) {
-                const float w = c_idct_basis[8 * y + v];
-                a0[y] = __fadd_rn(a0[y], __fmul_rn(w, t0));
-                a1[y] = __fadd_rn(a1[y], __fmul_rn(w, t1));
+            for (int i = 0; i < 4; i++) {
+                const uint64_t w = idct_pair(4u * v + i);
+                a0[i] = pair_add(a0[i], pair_mul(w, d0));
+                a1[i] = pair_add(a1[i], pair_mul(w, d1));
             }
         }
+        const uint64_t os2 = pair_of(oscale, oscale), ob2 = pair_of(obias, obias);
         uint32_t *dst = stage + start_of(c) / 2u + j * nb + blk;
 #pragma unroll
-        for (int y = 0; y < 8; y++) dst[4u * y * nb] = convert(a0[y]) | (convert(a1[y]) << 16);
+        for (int i = 0; i < 4; i++) {
+            float p0, p1, q0, q1;
+            pair_split(pair_add(pair_mul(a0[i], os2), ob2), p0, p1);
+            pair_split(pair_add(pair_mul(a1[i], os2), ob2), q0, q1);
+            dst[4u * (2 * i) * nb] = convert(p0) | (convert(q0) << 16);
+            dst[4u * (2 * i + 1) * nb] = convert(p1) | (convert(q1) << 16);
+        }
     }
     __syncthreads();
 
@@ -914,13 +937,6 @@ __device__ __forceinline__ float small_int_to_float(int32_t q) {
     return __fadd_rn(__int_as_float(0x4B400000 + q), -12582912.0f);
 }
 
-// floor(v) clamped to [0, max] (max an integer below 2^16), as an integer:
-// clamping before the floor gives the same value as after it for integer
-// bounds, and adding 2^23 rounded down leaves floor(v) in the low bits.
-__device__ __forceinline__ uint32_t floor_clamped(float v, float max) {
-    const float c = fminf(fmaxf(v, 0.0f), max);
-    return __float_as_uint(__fadd_rd(c, 8388608.0f)) & 0xFFFFu;
-}
 
 // One block: dequantise (F = QF scale, src/dsp/scalar.rs:8-12), the IDCT's
 // row pass tmp[v][x] = sum_u F[v][u] T[x][u] and column pass
@@ -1229,6 +1245,13 @@ cudaError_t configure_decode_kernels() {
     float basis[64];
     dct_basis(basis);
     if ((e = cudaMemcpyToSymbol(c_idct_basis, basis, sizeof basis)) != cudaSuccess) return e;
+    float pairs[64];
+    for (int u = 0; u < 8; u++)
+        for (int j = 0; j < 4; j++) {
+            pairs[2 * (4 * u + j)] = basis[8 * (2 * j) + u];
+            pairs[2 * (4 * u + j) + 1] = basis[8 * (2 * j + 1) + u];
+        }
+    if ((e = cudaMemcpyToSymbol(c_idct_pairs, pairs, sizeof pairs)) != cudaSuccess) return e;
     return upload_scans();
 }
 

@@ -925,7 +925,8 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
 // proportion to its macroblocks, plus a quarter, plus one step (its size
 // change at the first finer quantiser), and never above the most its share
 // can come to (the crate's prefetch rule: the whole slack from the slice on,
-// if no slice before it took any). The share-out's allowance for a slice is
+// if no slice before it took any); for a slice whose step is under a
+// quarter of its share, it is that most. The share-out's allowance for a slice is
 // what the slices before it left, which stays near the proportional share
 // but for the last few slices of a picture; the most is far above it there
 // (the last slice's is the whole slack), and a ladder to the most costed
@@ -961,7 +962,10 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
             const uint64_t n1 = slice_total(hb, cc, alpha, f1);
             step = n1 > used ? n1 - used : 0u;
         }
-        const uint64_t likely = min(most, used + share + share / 4u + step);
+        // A slice whose first step is small beside its share (a coarse
+        // quantiser, where a step often changes no size) walks many levels
+        // wherever its allowance lands: its ladder goes to the most.
+        const uint64_t likely = 4u * step <= share ? most : min(most, used + share + share / 4u + step);
         const uint32_t *c = level_comp(e, st, kWindow - 1, s);
         bool fits = false;
         uint64_t n = ~0ull;
