@@ -31,12 +31,9 @@ namespace prores {
 
 __constant__ uint8_t c_scan[2][64];
 __constant__ float c_idct_basis[64];  // T[x][u] (dct_basis)
-// The basis as pairs down a column: idct_pair(4 u + j) = (T[2 j][u], T[2 j + 1][u]).
-__constant__ __align__(16) float c_idct_pairs[64];
 
 namespace {
 
-__device__ __forceinline__ uint64_t idct_pair(uint32_t k) { return reinterpret_cast<const uint64_t *>(c_idct_pairs)[k]; }
 
 // floor(v) clamped to [0, max] (max an integer below 2^16), as an integer:
 // clamping before the floor gives the same value as after it for integer
@@ -274,9 +271,11 @@ __device__ __forceinline__ bool window_code(uint32_t t, Codebook cb, uint32_t &s
 // reader would read them). A longer codeword and the last bits of the data
 // go through the general reader, which also names every failure as the
 // crate does.
+// The DC part of decode_scanned() (src/decode.rs:486-498): the first
+// DC by EG5, each next one as a difference by Table 9 on the previous
+// difference, the sign flipped after a negative one.
 template <class Out>
-__device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
-                                const uint16_t *level_tab) {
+__device__ int decode_dc(Bits &b, uint32_t n_blocks, Out &out) {
     uint32_t sym;
     int err = read_sym(b, nullptr, kFirstDcBook, sym);
     if (err) return err;
@@ -293,6 +292,14 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
         out.put(i, prev_dc);
         prev_diff = diff;
     }
+    return DE_OK;
+}
+
+template <class Out>
+__device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
+                                const uint16_t *level_tab) {
+    int err = decode_dc(b, n_blocks, out);
+    if (err) return err;
     const uint32_t total = n_blocks * 64;
     uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
     // One run, level and sign an iteration: from the window while it holds
@@ -497,10 +504,15 @@ __device__ int2 component_range(const uint8_t *sb, uint32_t size, bool has_alpha
     return make_int2(DE_OK, 0);
 }
 
-// One work item: component `comp` (0 Y', 1 Cb, 2 Cr, 3 alpha) of slice `s`.
-__device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, const uint16_t *run_tab,
-                            const uint16_t *level_tab) {
+// The DC pass over one work item, component `comp` (0 Y', 1 Cb, 2 Cr, 3
+// alpha) of slice `s`: the slice header, then the component's DC codes
+// into its coefficient list, and where its AC codes start (for the AC
+// pass, which writes the count and status of a component that gets that
+// far); an alpha component is decoded whole. A failure is written here.
+__device__ void decode_item_dc(const DecodeLaunch &d, uint32_t comp, uint32_t s) {
     int2 *slot = d.slot_status + 4ull * s + comp;
+    AcStart *rec = comp < 3 ? d.ac_start + (uint64_t)comp * d.n_slices + s : nullptr;
+    if (rec) rec->meta = 0;
     const SliceDesc sd = d.slices[s];
     const PicDesc &pd = d.pics[sd.pic];
     if (d.pic_status[sd.pic].locate_slice >= 0) return;  // never read: the picture failed before decoding
@@ -521,19 +533,165 @@ __device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, co
     }
     Bits b;
     b.init(d.bits, sd.off + start, len);
-    int err;
     if (comp == 3) {
-        err = decode_alpha(b, fd, pd, sd, d.alpha);
-    } else {
-        const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
-        const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
-        const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
-        CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u, 0u};
-        err = decode_component(b, n_blocks, list, run_tab, level_tab);
-        d.coef_count[3ull * s + comp] = list.count;
+        *slot = make_int2(decode_alpha(b, fd, pd, sd, d.alpha), 0);
+        return;
     }
-    *slot = make_int2(err, 0);
+    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+    const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
+    const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
+    CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u, 0u};
+    const int err = decode_dc(b, n_blocks, list);
+    if (err) {
+        d.coef_count[3ull * s + comp] = list.count;
+        *slot = make_int2(err, 0);
+        return;
+    }
+    AcStart r;
+    r.pos = b.pos;
+    r.coef_off = base;
+    r.left = (uint32_t)(b.end - b.pos);
+    r.meta = AcStart::kAcLive | (n_blocks << 8) | list.big;
+    *rec = r;
 }
+
+// The AC pass's state for the component a lane decodes: the codes of
+// decode_component()'s AC loop, one run, level and sign a step, so that a
+// lane that finishes its component takes the next one at once instead of
+// waiting for the slowest lane of its warp.
+struct AcLane {
+    CoefList list;
+    Bits b;
+    Window win;
+    uint32_t n, total, prev_run, prev_level, rrow, lrow;
+    bool in_win;
+
+    __device__ __forceinline__ void start(const DecodeLaunch &d, const AcStart &r) {
+        const uint32_t n_blocks = (r.meta >> 8) & 0xFFu;
+        list = CoefList{reinterpret_cast<uint32_t *>(d.coef + r.coef_off), 64u * n_blocks, r.meta & 0xFFu, n_blocks};
+        b.w = reinterpret_cast<const uint64_t *>(d.bits);
+        b.pos = r.pos;
+        b.end = r.pos + r.left;
+        b.idx = ~0ull - 1u;  // no words held: the first peek loads them
+        n = n_blocks;
+        total = 64u * n_blocks;
+        prev_run = 4;
+        prev_level = 1;
+        rrow = run_book_row(prev_run) * kDecodeEntries;
+        lrow = level_book_row(prev_level) * kDecodeEntries;
+        in_win = r.left >= 32u;
+        if (in_win) win.init(d.bits, b.pos, b.end);
+    }
+
+    // One step; true when the component is done, with its status in `err`.
+    __device__ __forceinline__ bool step(const uint16_t *run_tab, const uint16_t *level_tab, int &err) {
+        bool level_next = false;  // the run is read; its level and sign are the general reader's
+        if (in_win && win.left >= 32u) {
+            const uint32_t t = win.top();
+            const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
+            uint32_t run = 0, l = 0;
+            bool got = true;
+            if (e1) {
+                l = e1 & 15u;
+                run = (e1 >> 4) & 63u;
+                const uint32_t t2 = t << l;
+                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
+                if (e2) {
+                    // Run, level and sign in one go.
+                    const uint32_t l2 = e2 & 15u;
+                    prev_run = run;
+                    prev_level = (e2 >> 4) & 63u;
+                    n += run;
+                    if (n >= total) {
+                        err = DE_RUN_PAST_END;
+                        return true;
+                    }
+                    const int32_t level = (int32_t)prev_level + 1;
+                    list.put(n, (t2 << l2) >> 31 ? -level : level);
+                    n += 1;
+                    rrow = (e1 >> 10) * kDecodeEntries;
+                    lrow = (e2 >> 10) * kDecodeEntries;
+                    win.consume(l + l2 + 1u);
+                    return false;
+                }
+            } else {
+                got = window_code(t, run_book(prev_run), run, l);
+            }
+            if (got) {
+                prev_run = run;
+                n += run;
+                if (n >= total) {
+                    err = DE_RUN_PAST_END;
+                    return true;
+                }
+                win.consume(l);
+                uint32_t lvl = 0;
+                got = false;
+                if (win.left >= 32u) {
+                    const uint32_t u = win.top();
+                    const uint32_t e2 = level_tab[lrow + (u >> (32 - kDecodeBits))];
+                    if (e2) {
+                        lvl = (e2 >> 4) & 63u;
+                        l = e2 & 15u;
+                        got = true;
+                    } else {
+                        got = window_code(u, level_book(prev_level), lvl, l);
+                    }
+                }
+                if (got) {
+                    win.consume(l);
+                    prev_level = lvl;
+                    if (win.left == 0) {
+                        err = DE_PAST_END;
+                        return true;
+                    }
+                    const bool neg = win.top() >> 31;
+                    win.consume(1u);
+                    const int32_t level = (int32_t)lvl + 1;
+                    list.put(n, neg ? -level : level);
+                    n += 1;
+                    rrow = run_book_row(prev_run) * kDecodeEntries;
+                    lrow = level_book_row(prev_level) * kDecodeEntries;
+                    return false;
+                }
+                level_next = true;
+            }
+        }
+        // The general reader, from the window's position.
+        if (in_win) b.pos = b.end - win.left;
+        if (!level_next) {
+            if (b.remaining() <= 31 && b.peek() == 0) {  // endOfData()
+                err = DE_OK;
+                return true;
+            }
+            uint32_t run;
+            if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return true;
+            prev_run = run;
+            n += run;
+            if (n >= total) {
+                err = DE_RUN_PAST_END;
+                return true;
+            }
+        }
+        uint32_t lvl;
+        if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return true;
+        prev_level = lvl;
+        if (b.remaining() < 1) {
+            err = DE_PAST_END;
+            return true;
+        }
+        const bool neg = b.peek() >> 63;
+        b.pos += 1;
+        const int32_t level = (int32_t)lvl + 1;
+        list.put(n, neg ? -level : level);
+        n += 1;
+        rrow = run_book_row(prev_run) * kDecodeEntries;
+        lrow = level_book_row(prev_level) * kDecodeEntries;
+        in_win = b.remaining() >= 32;
+        if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
+        return false;
+    }
+};
 
 // ------------------------------------------------------------------ kernels
 
@@ -630,10 +788,24 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate(DecodeLaunch d) {
 }
 
 constexpr int kEntropyMaxThreads = 512;
+constexpr int kEntropyDcThreads = 256;
 
-// Persistent: each warp takes 32 x entropy_per_lane slice components per
-// grab of the work counter, a lane each in turn, component-major, until the
-// list runs out.
+// The DC pass: a thread per work item (component-major, so the threads of
+// a warp take the same component of neighbouring slices, whose DC parts
+// have the same number of codes).
+__global__ void __launch_bounds__(kEntropyDcThreads) k_entropy_dc(DecodeLaunch d) {
+    const uint32_t items = 4u * d.n_slices;
+    const uint32_t item = blockIdx.x * kEntropyDcThreads + threadIdx.x;
+    if (item >= items) return;
+    const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
+    decode_item_dc(d, comp, s);
+}
+
+// The AC pass, persistent: a lane decodes one slice component's AC codes a
+// step at a time and, when it is done, takes the next component at once
+// (the lanes of a warp that need one share a grab of the work counter), so
+// the lanes of a warp stay busy until the list runs out. Components are
+// taken in the DC pass's order.
 __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) {
     __shared__ uint16_t run_tab[kBookTableWords];
     __shared__ uint16_t level_tab[kBookTableWords];
@@ -642,23 +814,45 @@ __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) 
         reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_books)[i];
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint32_t items = 4u * d.n_slices;
-    const uint32_t per_lane = d.entropy_per_lane > 0 ? d.entropy_per_lane : 1u;
-    const uint32_t grab = 32u * per_lane;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t items = 3u * d.n_slices;
+    unsigned int *counter = d.work_counter + 1;
+    AcLane st;
+    bool busy = false, drained = false;
+    uint32_t item = 0;
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(d.work_counter, grab);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= items) break;
-        for (uint32_t k = 0; k < per_lane; k++) {
-            const uint32_t item = base + 32u * k + lane;
-            if (item < items) {
-                const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
-                decode_item(d, comp, s, run_tab, level_tab);
+        const uint32_t need = __ballot_sync(0xffffffffu, !busy && !drained);
+        if (need) {
+            const uint32_t leader = (uint32_t)__ffs(need) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(counter, (unsigned int)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!busy && !drained) {
+                item = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                if (item >= items) {
+                    drained = true;
+                } else {
+                    const AcStart r = d.ac_start[item];
+                    if (r.meta & AcStart::kAcLive) {
+                        st.start(d, r);
+                        busy = true;
+                    }
+                }
             }
         }
-        __syncwarp();
+        if (!__any_sync(0xffffffffu, busy)) {
+            if (__all_sync(0xffffffffu, drained)) break;
+            continue;
+        }
+        if (busy) {
+            int err = DE_OK;
+            if (st.step(run_tab, level_tab, err)) {
+                const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
+                d.coef_count[3ull * s + comp] = st.list.count;
+                d.slot_status[4ull * s + comp] = make_int2(err, 0);
+                busy = false;
+            }
+        }
     }
 }
 
@@ -762,15 +956,15 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         }
         held_any[k] = any;
         if (any) {
-            // Outputs x = 2 j, 2 j + 1 a pair, each sum in the same order.
-            uint64_t rr[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) rr[u] = pair_of(row[u], row[u]);
+            // Outputs x = 2 j, 2 j + 1 summed as a pair, each in the same
+            // order; the products stay scalar (see pair_math.h).
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 uint64_t acc = 0;
 #pragma unroll
-                for (int u = 0; u < 8; u++) acc = pair_add(acc, pair_mul(rr[u], idct_pair(4u * u + j)));
+                for (int u = 0; u < 8; u++)
+                    acc = pair_add(acc, pair_of(__fmul_rn(row[u], c_idct_basis[8 * (2 * j) + u]),
+                                                __fmul_rn(row[u], c_idct_basis[8 * (2 * j + 1) + u])));
                 pair_split(acc, held[k][2 * j], held[k][2 * j + 1]);
             }
         }
@@ -818,21 +1012,25 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         for (int v = 0; v < 8; v++) {
             if (!((rows >> (8 * v)) & 0xffu)) continue;
             const float t0 = src[8u * v * nb], t1 = src[8u * v * nb + nb];
-            const uint64_t d0 = pair_of(t0, t0), d1 = pair_of(t1, t1);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                const uint64_t w = idct_pair(4u * v + i);
-                a0[i] = pair_add(a0[i], pair_mul(w, d0));
-                a1[i] = pair_add(a1[i], pair_mul(w, d1));
+                const float w0 = c_idct_basis[8 * (2 * i) + v], w1 = c_idct_basis[8 * (2 * i + 1) + v];
+                a0[i] = pair_add(a0[i], pair_of(__fmul_rn(w0, t0), __fmul_rn(w1, t0)));
+                a1[i] = pair_add(a1[i], pair_of(__fmul_rn(w0, t1), __fmul_rn(w1, t1)));
             }
         }
-        const uint64_t os2 = pair_of(oscale, oscale), ob2 = pair_of(obias, obias);
+        const uint64_t ob2 = pair_of(obias, obias);
+        const auto scaled = [&](uint64_t a) {
+            float lo, hi;
+            pair_split(a, lo, hi);
+            return pair_add(pair_of(__fmul_rn(lo, oscale), __fmul_rn(hi, oscale)), ob2);
+        };
         uint32_t *dst = stage + start_of(c) / 2u + j * nb + blk;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             float p0, p1, q0, q1;
-            pair_split(pair_add(pair_mul(a0[i], os2), ob2), p0, p1);
-            pair_split(pair_add(pair_mul(a1[i], os2), ob2), q0, q1);
+            pair_split(scaled(a0[i]), p0, p1);
+            pair_split(scaled(a1[i]), q0, q1);
             dst[4u * (2 * i) * nb] = convert(p0) | (convert(q0) << 16);
             dst[4u * (2 * i + 1) * nb] = convert(p1) | (convert(q1) << 16);
         }
@@ -1182,6 +1380,10 @@ cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s) {
 
 cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cudaStream_t s) {
     if (d.n_slices == 0) return cudaSuccess;
+    const uint32_t items = 4u * d.n_slices;
+    k_entropy_dc<<<(items + kEntropyDcThreads - 1) / kEntropyDcThreads, kEntropyDcThreads, 0, s>>>(d);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     k_entropy<<<shape.grid, 32 * shape.warps_per_block, 0, s>>>(d);
     return cudaGetLastError();
 }
@@ -1245,13 +1447,6 @@ cudaError_t configure_decode_kernels() {
     float basis[64];
     dct_basis(basis);
     if ((e = cudaMemcpyToSymbol(c_idct_basis, basis, sizeof basis)) != cudaSuccess) return e;
-    float pairs[64];
-    for (int u = 0; u < 8; u++)
-        for (int j = 0; j < 4; j++) {
-            pairs[2 * (4 * u + j)] = basis[8 * (2 * j) + u];
-            pairs[2 * (4 * u + j) + 1] = basis[8 * (2 * j + 1) + u];
-        }
-    if ((e = cudaMemcpyToSymbol(c_idct_pairs, pairs, sizeof pairs)) != cudaSuccess) return e;
     return upload_scans();
 }
 

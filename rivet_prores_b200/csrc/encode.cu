@@ -35,6 +35,7 @@
 
 #include "codec_tables.h"
 #include "encode_types.h"
+#include "pair_math.h"
 
 namespace prores {
 
@@ -162,12 +163,16 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
                     p[x] = __fsub_rn(__fmul_rn((float)__ldg(line + col), scale), 256.0f);
                 }
             }
+            // Outputs u = 2 j, 2 j + 1 summed as a pair, each in the same
+            // order; the products stay scalar (see pair_math.h).
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
-                float acc = 0.0f;
+            for (int j = 0; j < 4; j++) {
+                uint64_t acc = 0;
 #pragma unroll
-                for (int x = 0; x < 8; x++) acc = __fadd_rn(acc, __fmul_rn(p[x], c_fdct_basis[8 * x + u]));
-                tmp[8 * y + u][lane] = acc;
+                for (int x = 0; x < 8; x++)
+                    acc = pair_add(acc, pair_of(__fmul_rn(p[x], c_fdct_basis[8 * x + 2 * j]),
+                                                __fmul_rn(p[x], c_fdct_basis[8 * x + 2 * j + 1])));
+                pair_split(acc, tmp[8 * y + 2 * j][lane], tmp[8 * y + 2 * j + 1][lane]);
             }
         }
         // Columns: F[v][u] = sum_y T[y][v] tmp[y][u], y in order from 0.
@@ -178,11 +183,20 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
             float col[8];
 #pragma unroll
             for (int y = 0; y < 8; y++) col[y] = tmp[8 * y + u][lane];
+            float res[8];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                // Outputs v = 2 j, 2 j + 1 summed as a pair.
+                uint64_t acc = 0;
+#pragma unroll
+                for (int y = 0; y < 8; y++)
+                    acc = pair_add(acc, pair_of(__fmul_rn(c_fdct_basis[8 * y + 2 * j], col[y]),
+                                                __fmul_rn(c_fdct_basis[8 * y + 2 * j + 1], col[y])));
+                pair_split(acc, res[2 * j], res[2 * j + 1]);
+            }
 #pragma unroll
             for (int v = 0; v < 8; v++) {
-                float acc = 0.0f;
-#pragma unroll
-                for (int y = 0; y < 8; y++) acc = __fadd_rn(acc, __fmul_rn(c_fdct_basis[8 * y + v], col[y]));
+                const float acc = res[v];
                 const uint32_t sp = scan[8 * v + u];
                 out[nb * sp + lane] = acc;
                 // Every active lane is at this position, in one chunk.

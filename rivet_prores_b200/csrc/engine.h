@@ -89,7 +89,8 @@ struct Workspace {
     int device = 0;
     uint32_t wait_ms = kDefaultWaitMs;  // the context's bound when the workspace was taken
     cudaStream_t stream = nullptr;
-    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter;
+    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter,
+        ac_start;
     // encode
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
