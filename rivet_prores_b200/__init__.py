@@ -350,7 +350,7 @@ class Tuning:
     entropy_blocks_per_sm: int = 0
     entropy_components_per_lane: int = 1
     staging_depth: int = 4
-    decode_fused: int = 1
+    decode_fused: int = 0
     decode_slot_positions: int = 65536
     decode_slot_bytes: int = 1
 

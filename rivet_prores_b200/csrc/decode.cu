@@ -504,15 +504,10 @@ __device__ int2 component_range(const uint8_t *sb, uint32_t size, bool has_alpha
     return make_int2(DE_OK, 0);
 }
 
-// The DC pass over one work item, component `comp` (0 Y', 1 Cb, 2 Cr, 3
-// alpha) of slice `s`: the slice header, then the component's DC codes
-// into its coefficient list, and where its AC codes start (for the AC
-// pass, which writes the count and status of a component that gets that
-// far); an alpha component is decoded whole. A failure is written here.
-__device__ void decode_item_dc(const DecodeLaunch &d, uint32_t comp, uint32_t s) {
+// One work item: component `comp` (0 Y', 1 Cb, 2 Cr, 3 alpha) of slice `s`.
+__device__ void decode_item(const DecodeLaunch &d, uint32_t comp, uint32_t s, const uint16_t *run_tab,
+                            const uint16_t *level_tab) {
     int2 *slot = d.slot_status + 4ull * s + comp;
-    AcStart *rec = comp < 3 ? d.ac_start + (uint64_t)comp * d.n_slices + s : nullptr;
-    if (rec) rec->meta = 0;
     const SliceDesc sd = d.slices[s];
     const PicDesc &pd = d.pics[sd.pic];
     if (d.pic_status[sd.pic].locate_slice >= 0) return;  // never read: the picture failed before decoding
@@ -533,165 +528,19 @@ __device__ void decode_item_dc(const DecodeLaunch &d, uint32_t comp, uint32_t s)
     }
     Bits b;
     b.init(d.bits, sd.off + start, len);
+    int err;
     if (comp == 3) {
-        *slot = make_int2(decode_alpha(b, fd, pd, sd, d.alpha), 0);
-        return;
-    }
-    const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
-    const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
-    const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
-    CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u, 0u};
-    const int err = decode_dc(b, n_blocks, list);
-    if (err) {
+        err = decode_alpha(b, fd, pd, sd, d.alpha);
+    } else {
+        const uint32_t cpm = fd.chroma == 2 ? 2u : 4u;
+        const uint32_t n_blocks = (comp == 0 ? 4u : cpm) * sd.mbs;
+        const uint64_t base = sd.coef + (comp == 0 ? 0ull : 64ull * sd.mbs * (4u + (comp - 1u) * cpm));
+        CoefList list{reinterpret_cast<uint32_t *>(d.coef + base), 64u * n_blocks, 0u, 0u};
+        err = decode_component(b, n_blocks, list, run_tab, level_tab);
         d.coef_count[3ull * s + comp] = list.count;
-        *slot = make_int2(err, 0);
-        return;
     }
-    AcStart r;
-    r.pos = b.pos;
-    r.coef_off = base;
-    r.left = (uint32_t)(b.end - b.pos);
-    r.meta = AcStart::kAcLive | (n_blocks << 8) | list.big;
-    *rec = r;
+    *slot = make_int2(err, 0);
 }
-
-// The AC pass's state for the component a lane decodes: the codes of
-// decode_component()'s AC loop, one run, level and sign a step, so that a
-// lane that finishes its component takes the next one at once instead of
-// waiting for the slowest lane of its warp.
-struct AcLane {
-    CoefList list;
-    Bits b;
-    Window win;
-    uint32_t n, total, prev_run, prev_level, rrow, lrow;
-    bool in_win;
-
-    __device__ __forceinline__ void start(const DecodeLaunch &d, const AcStart &r) {
-        const uint32_t n_blocks = (r.meta >> 8) & 0xFFu;
-        list = CoefList{reinterpret_cast<uint32_t *>(d.coef + r.coef_off), 64u * n_blocks, r.meta & 0xFFu, n_blocks};
-        b.w = reinterpret_cast<const uint64_t *>(d.bits);
-        b.pos = r.pos;
-        b.end = r.pos + r.left;
-        b.idx = ~0ull - 1u;  // no words held: the first peek loads them
-        n = n_blocks;
-        total = 64u * n_blocks;
-        prev_run = 4;
-        prev_level = 1;
-        rrow = run_book_row(prev_run) * kDecodeEntries;
-        lrow = level_book_row(prev_level) * kDecodeEntries;
-        in_win = r.left >= 32u;
-        if (in_win) win.init(d.bits, b.pos, b.end);
-    }
-
-    // One step; true when the component is done, with its status in `err`.
-    __device__ __forceinline__ bool step(const uint16_t *run_tab, const uint16_t *level_tab, int &err) {
-        bool level_next = false;  // the run is read; its level and sign are the general reader's
-        if (in_win && win.left >= 32u) {
-            const uint32_t t = win.top();
-            const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
-            uint32_t run = 0, l = 0;
-            bool got = true;
-            if (e1) {
-                l = e1 & 15u;
-                run = (e1 >> 4) & 63u;
-                const uint32_t t2 = t << l;
-                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
-                if (e2) {
-                    // Run, level and sign in one go.
-                    const uint32_t l2 = e2 & 15u;
-                    prev_run = run;
-                    prev_level = (e2 >> 4) & 63u;
-                    n += run;
-                    if (n >= total) {
-                        err = DE_RUN_PAST_END;
-                        return true;
-                    }
-                    const int32_t level = (int32_t)prev_level + 1;
-                    list.put(n, (t2 << l2) >> 31 ? -level : level);
-                    n += 1;
-                    rrow = (e1 >> 10) * kDecodeEntries;
-                    lrow = (e2 >> 10) * kDecodeEntries;
-                    win.consume(l + l2 + 1u);
-                    return false;
-                }
-            } else {
-                got = window_code(t, run_book(prev_run), run, l);
-            }
-            if (got) {
-                prev_run = run;
-                n += run;
-                if (n >= total) {
-                    err = DE_RUN_PAST_END;
-                    return true;
-                }
-                win.consume(l);
-                uint32_t lvl = 0;
-                got = false;
-                if (win.left >= 32u) {
-                    const uint32_t u = win.top();
-                    const uint32_t e2 = level_tab[lrow + (u >> (32 - kDecodeBits))];
-                    if (e2) {
-                        lvl = (e2 >> 4) & 63u;
-                        l = e2 & 15u;
-                        got = true;
-                    } else {
-                        got = window_code(u, level_book(prev_level), lvl, l);
-                    }
-                }
-                if (got) {
-                    win.consume(l);
-                    prev_level = lvl;
-                    if (win.left == 0) {
-                        err = DE_PAST_END;
-                        return true;
-                    }
-                    const bool neg = win.top() >> 31;
-                    win.consume(1u);
-                    const int32_t level = (int32_t)lvl + 1;
-                    list.put(n, neg ? -level : level);
-                    n += 1;
-                    rrow = run_book_row(prev_run) * kDecodeEntries;
-                    lrow = level_book_row(prev_level) * kDecodeEntries;
-                    return false;
-                }
-                level_next = true;
-            }
-        }
-        // The general reader, from the window's position.
-        if (in_win) b.pos = b.end - win.left;
-        if (!level_next) {
-            if (b.remaining() <= 31 && b.peek() == 0) {  // endOfData()
-                err = DE_OK;
-                return true;
-            }
-            uint32_t run;
-            if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return true;
-            prev_run = run;
-            n += run;
-            if (n >= total) {
-                err = DE_RUN_PAST_END;
-                return true;
-            }
-        }
-        uint32_t lvl;
-        if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return true;
-        prev_level = lvl;
-        if (b.remaining() < 1) {
-            err = DE_PAST_END;
-            return true;
-        }
-        const bool neg = b.peek() >> 63;
-        b.pos += 1;
-        const int32_t level = (int32_t)lvl + 1;
-        list.put(n, neg ? -level : level);
-        n += 1;
-        rrow = run_book_row(prev_run) * kDecodeEntries;
-        lrow = level_book_row(prev_level) * kDecodeEntries;
-        in_win = b.remaining() >= 32;
-        if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
-        return false;
-    }
-};
 
 // ------------------------------------------------------------------ kernels
 
@@ -788,24 +637,10 @@ __global__ void __launch_bounds__(kLocateThreads) k_locate(DecodeLaunch d) {
 }
 
 constexpr int kEntropyMaxThreads = 512;
-constexpr int kEntropyDcThreads = 256;
 
-// The DC pass: a thread per work item (component-major, so the threads of
-// a warp take the same component of neighbouring slices, whose DC parts
-// have the same number of codes).
-__global__ void __launch_bounds__(kEntropyDcThreads) k_entropy_dc(DecodeLaunch d) {
-    const uint32_t items = 4u * d.n_slices;
-    const uint32_t item = blockIdx.x * kEntropyDcThreads + threadIdx.x;
-    if (item >= items) return;
-    const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
-    decode_item_dc(d, comp, s);
-}
-
-// The AC pass, persistent: a lane decodes one slice component's AC codes a
-// step at a time and, when it is done, takes the next component at once
-// (the lanes of a warp that need one share a grab of the work counter), so
-// the lanes of a warp stay busy until the list runs out. Components are
-// taken in the DC pass's order.
+// Persistent: each warp takes 32 x entropy_per_lane slice components per
+// grab of the work counter, a lane each in turn, component-major, until the
+// list runs out.
 __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) {
     __shared__ uint16_t run_tab[kBookTableWords];
     __shared__ uint16_t level_tab[kBookTableWords];
@@ -814,45 +649,23 @@ __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) 
         reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_books)[i];
     }
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t items = 3u * d.n_slices;
-    unsigned int *counter = d.work_counter + 1;
-    AcLane st;
-    bool busy = false, drained = false;
-    uint32_t item = 0;
+    const int lane = threadIdx.x & 31;
+    const uint32_t items = 4u * d.n_slices;
+    const uint32_t per_lane = d.entropy_per_lane > 0 ? d.entropy_per_lane : 1u;
+    const uint32_t grab = 32u * per_lane;
     for (;;) {
-        const uint32_t need = __ballot_sync(0xffffffffu, !busy && !drained);
-        if (need) {
-            const uint32_t leader = (uint32_t)__ffs(need) - 1u;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(counter, (unsigned int)__popc(need));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (!busy && !drained) {
-                item = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
-                if (item >= items) {
-                    drained = true;
-                } else {
-                    const AcStart r = d.ac_start[item];
-                    if (r.meta & AcStart::kAcLive) {
-                        st.start(d, r);
-                        busy = true;
-                    }
-                }
-            }
-        }
-        if (!__any_sync(0xffffffffu, busy)) {
-            if (__all_sync(0xffffffffu, drained)) break;
-            continue;
-        }
-        if (busy) {
-            int err = DE_OK;
-            if (st.step(run_tab, level_tab, err)) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(d.work_counter, grab);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= items) break;
+        for (uint32_t k = 0; k < per_lane; k++) {
+            const uint32_t item = base + 32u * k + lane;
+            if (item < items) {
                 const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
-                d.coef_count[3ull * s + comp] = st.list.count;
-                d.slot_status[4ull * s + comp] = make_int2(err, 0);
-                busy = false;
+                decode_item(d, comp, s, run_tab, level_tab);
             }
         }
+        __syncwarp();
     }
 }
 
@@ -1380,10 +1193,6 @@ cudaError_t launch_locate(const DecodeLaunch &d, cudaStream_t s) {
 
 cudaError_t launch_entropy(const DecodeLaunch &d, const EntropyShape &shape, cudaStream_t s) {
     if (d.n_slices == 0) return cudaSuccess;
-    const uint32_t items = 4u * d.n_slices;
-    k_entropy_dc<<<(items + kEntropyDcThreads - 1) / kEntropyDcThreads, kEntropyDcThreads, 0, s>>>(d);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
     k_entropy<<<shape.grid, 32 * shape.warps_per_block, 0, s>>>(d);
     return cudaGetLastError();
 }

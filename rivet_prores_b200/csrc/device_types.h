@@ -83,16 +83,6 @@ struct DeviceTables {
     float *basis;            // T[x][u] at 8x + u, as the crate computes it
 };
 
-// Where the AC codes of a slice component start, found by the DC pass of
-// the two-kernel decode (k_entropy_dc) for the AC pass (k_entropy).
-struct AcStart {
-    uint64_t pos;       // bit position of the first AC code in the bitstream buffer
-    uint64_t coef_off;  // the component's coefficient list: offset into DecodeLaunch::coef
-    uint32_t left;      // bits of the component from pos on
-    uint32_t meta;      // kAcLive | n_blocks << 8 | large values the DC part put at the list's back
-    static constexpr uint32_t kAcLive = 0x80000000u;  // the AC pass decodes it (else nothing to do)
-};
-
 struct DecodeLaunch {
     const uint8_t *bits;  // bitstream buffer (64 bytes of zero padding after the end)
     uint64_t bits_len;
@@ -112,8 +102,7 @@ struct DecodeLaunch {
     uint16_t *planes;
     uint16_t *alpha;
     const uint8_t *weights;  // [set][2][64] raster weights
-    unsigned int *work_counter;  // [0] the fused decode's or the DC pass's, [1] the AC pass's
-    AcStart *ac_start;           // [3 n_slices], component-major (two-kernel decode)
+    unsigned int *work_counter;
     uint32_t n_frames, n_pics, n_slices;
     uint32_t entropy_per_lane;  // slice components a lane decodes per grab of the work counter
     // Fused decode: slices a CTA takes at once, and the coefficient

@@ -767,20 +767,33 @@ __device__ __forceinline__ uint32_t warp_component_bytes(const EncodeLaunch &e, 
 constexpr int kCostThreads = 256;
 
 // Work items are (component, slice), component-major: a warp's lanes take
-// the same component of 32 neighbouring slices, which cost about the same.
+// the same component of 32 neighbouring slices, which cost about the same
+// (and whose zero chunks mostly coincide, so the lanes skip them together).
+// Persistent: as many CTAs as are resident, each warp taking 32 items at a
+// time from the probe's counter, so no warp waits for the slowest of its
+// CTA and the last wave is not left part-empty.
 __global__ void __launch_bounds__(kCostThreads) k_cost(EncodeLaunch e, int step) {
     __shared__ LenTables t;
     t.fill();
     __syncthreads();
-    const uint32_t item = blockIdx.x * kCostThreads + threadIdx.x;
-    if (item >= 3u * e.n_slices) return;
-    const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
-    const EncSliceDesc sd = e.slices[s];
-    const int32_t qi = e.state[sd.pic].probe_qi;
-    if (qi == 0) return;
-    const EncPicDesc &pd = e.pics[sd.pic];
-    const EncFrameDesc &fd = e.frames[pd.frame];
-    e.probe_comp[((uint64_t)step * e.n_slices + s) * 3u + comp] = component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t items = 3u * e.n_slices;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(e.cost_taken + step, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= items) break;
+        const uint32_t item = base + lane;
+        if (item >= items) continue;
+        const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
+        const EncSliceDesc sd = e.slices[s];
+        const int32_t qi = e.state[sd.pic].probe_qi;
+        if (qi == 0) continue;
+        const EncPicDesc &pd = e.pics[sd.pic];
+        const EncFrameDesc &fd = e.frames[pd.frame];
+        e.probe_comp[((uint64_t)step * e.n_slices + s) * 3u + comp] =
+            component_bytes(e, sd, pd, fd, comp, (uint32_t)qi, t);
+    }
 }
 
 // k_cost with a warp per item, for batches too small to fill the GPU with
@@ -1037,8 +1050,10 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_init(EncodeLaunch e) {
         st.fits_at_all = 0;
         st.uniform = 224;
         e.state[blockIdx.x] = st;
-        if (blockIdx.x == 0)
+        if (blockIdx.x == 0) {
             for (int j = 0; j < kWindow; j++) e.win_count[j] = 0;
+            for (int j = 0; j < kProbeSteps; j++) e.cost_taken[j] = 0;
+        }
     }
 }
 
@@ -1677,9 +1692,17 @@ static bool lane_mode(const EncodeLaunch &e) {
 cudaError_t launch_cost(const EncodeLaunch &e, int step, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
     const uint32_t items = 3u * e.n_slices;
-    if (lane_mode(e))
-        k_cost<<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e, step);
-    else
+    if (lane_mode(e)) {
+        static int per_sm = 0;  // resident CTAs of k_cost per SM (the same for every device of a build)
+        if (per_sm == 0) {
+            int fit = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_cost, kCostThreads, 0);
+            per_sm = fit > 0 ? fit : 1;
+        }
+        const uint32_t need = (items + kCostThreads - 1) / kCostThreads;
+        const uint32_t grid = std::min<uint32_t>(need, (uint32_t)(per_sm * e.sm_count));
+        k_cost<<<grid, kCostThreads, 0, s>>>(e, step);
+    } else
         k_cost_warp<<<(items + kCostThreads / 32 - 1) / (kCostThreads / 32), kCostThreads, 0, s>>>(e, step);
     return cudaGetLastError();
 }

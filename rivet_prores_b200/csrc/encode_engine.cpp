@@ -313,6 +313,8 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
     e.win_list = reinterpret_cast<uint32_t *>(base + o);
     o += 4 * ns;
     e.win_count = reinterpret_cast<uint32_t *>(base + o);
+    o += 4 * kWindow;
+    e.cost_taken = reinterpret_cast<uint32_t *>(base + o);
     e.out = ws.enc_out.as<uint32_t>();
     e.headers = ws.enc_frame_out.as<uint8_t>();
     e.frame_status = ws.enc_alpha_bits.as<uint32_t>();
@@ -329,7 +331,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
 static size_t cost_bytes(const EncodePlan &plan) {
     const size_t ns = plan.n_slices + 1;
     return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 4 * ns +
-           4 * ns + sizeof(uint2) * kDeepLevels * ns + 4 * kWindow + 256;
+           4 * ns + sizeof(uint2) * kDeepLevels * ns + 4 * kWindow + 4 * kProbeSteps + 256;
 }
 
 static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s,

@@ -232,7 +232,7 @@ cudaError_t Stager::finish() {
 
 void Workspace::bind_stream() {
     for (DeviceBuf *b : {&bits, &frames, &pics, &slices, &slot_status, &pic_status, &coef, &coef_count, &planes,
-                         &alpha, &weights, &counter, &ac_start, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost, &enc_pic_state,
+                         &alpha, &weights, &counter, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost, &enc_pic_state,
                          &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes, &enc_frame_out}) {
         b->stream = stream;
         b->wait_ms = wait_ms;
@@ -516,7 +516,6 @@ Status upload_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaSt
     PR_CUDA(ws.counter.reserve(64), "cudaMalloc");
     PR_CUDA(ws.coef.reserve(8 * (plan.coef_total + 64)), "cudaMalloc coefficient lists");
     PR_CUDA(ws.coef_count.reserve(4 * 3 * ((size_t)plan.n_slices + 1)), "cudaMalloc");
-    PR_CUDA(ws.ac_start.reserve(sizeof(AcStart) * 3 * ((size_t)plan.n_slices + 1)), "cudaMalloc");
     if (!plan.fdesc.empty())
         PR_CUDA(ws.stager.h2d(ws.frames.p, plan.fdesc.data(), sizeof(FrameDesc) * plan.fdesc.size(), s),
                 "upload");
@@ -560,7 +559,6 @@ DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan 
     d.alpha = ws.alpha.as<uint16_t>();
     d.weights = ws.weights.as<uint8_t>();
     d.work_counter = ws.counter.as<unsigned int>();
-    d.ac_start = ws.ac_start.as<AcStart>();
     d.n_frames = (uint32_t)plan.fdesc.size();
     d.n_pics = (uint32_t)plan.pdesc.size();
     d.n_slices = plan.n_slices;
@@ -574,7 +572,7 @@ DecodeLaunch decode_launch_params(Context &ctx, Workspace &ws, const DecodePlan 
 
 Status enqueue_decode(Context &ctx, Workspace &ws, const DecodePlan &plan, cudaStream_t s, KernelTimes *kt) {
     const DecodeLaunch d = decode_launch_params(ctx, ws, plan);
-    PR_CUDA(cudaMemsetAsync(d.work_counter, 0, 2 * sizeof(unsigned int), s), "memset");
+    PR_CUDA(cudaMemsetAsync(d.work_counter, 0, sizeof(unsigned int), s), "memset");
     Status st;
     if ((st = record_kernel(kt, "start", s))) return st;
     PR_CUDA(launch_locate(d, s), "k_locate");

@@ -89,8 +89,7 @@ struct Workspace {
     int device = 0;
     uint32_t wait_ms = kDefaultWaitMs;  // the context's bound when the workspace was taken
     cudaStream_t stream = nullptr;
-    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter,
-        ac_start;
+    DeviceBuf bits, frames, pics, slices, slot_status, pic_status, coef, coef_count, planes, alpha, weights, counter;
     // encode
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
@@ -119,7 +118,7 @@ struct Tuning {
     int entropy_blocks_per_sm = 0;
     int entropy_components_per_lane = 1;
     int staging_depth = 4;
-    int decode_fused = 1;               // one kernel for the per-slice decode (else entropy, then IDCT)
+    int decode_fused = 0;               // one kernel for the per-slice decode (else entropy, then IDCT)
     int decode_slot_positions = 65536;  // coefficient positions a CTA of the fused decode holds
     int decode_slot_bytes = 1;          // bytes a coefficient takes there (1: int8, 2: int16)
 };
