@@ -772,7 +772,7 @@ constexpr int kCostThreads = 256;
 // Persistent: as many CTAs as are resident, each warp taking 32 items at a
 // time from the probe's counter, so no warp waits for the slowest of its
 // CTA and the last wave is not left part-empty.
-__global__ void __launch_bounds__(kCostThreads) k_cost(EncodeLaunch e, int step) {
+__global__ void __launch_bounds__(kCostThreads, 6) k_cost(EncodeLaunch e, int step) {
     __shared__ LenTables t;
     t.fill();
     __syncthreads();
@@ -960,6 +960,9 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
 // several quantisers of every slice of a picture's tail for nothing. What
 // the ladder leaves out only moves work to the share-out, never changes a
 // size.
+constexpr uint32_t kTailSlices = 64;  // a picture's tail: slices within this many slices' macroblocks of its end
+constexpr uint32_t kTailLevels = 8;
+
 __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
     __shared__ LenTables t;
     t.fill();
@@ -991,8 +994,13 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
         }
         // A slice whose first step is small beside its share (a coarse
         // quantiser, where a step often changes no size) walks many levels
-        // wherever its allowance lands: its ladder goes to the most.
-        const uint64_t likely = 4u * step <= share ? most : min(most, used + share + share / 4u + step);
+        // wherever its allowance lands: its ladder goes to the most. So do
+        // the last slices of a picture, where what the slices before left
+        // gathers, for at most kTailLevels levels.
+        const bool coarse = 4u * step <= share;
+        const bool tail = mbs_from(pd, sd) <= (uint64_t)kTailSlices * sd.mbs;
+        const uint64_t likely = coarse || tail ? most : min(most, used + share + share / 4u + step);
+        const uint32_t levels = coarse ? (uint32_t)kDeepLevels : (tail ? kTailLevels : (uint32_t)kDeepLevels);
         const uint32_t *c = level_comp(e, st, kWindow - 1, s);
         bool fits = false;
         uint64_t n = ~0ull;
@@ -1000,7 +1008,7 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
             const uint32_t cc[3] = {c[0], c[1], c[2]};
             n = slice_total(hb, cc, alpha, fits);
         }
-        for (uint32_t j = 0; fits && n <= likely && j < (uint32_t)kDeepLevels; j++) {
+        for (uint32_t j = 0; fits && n <= likely && j < levels; j++) {
             const int32_t qi = st.uniform - 1 - kWindow - (int32_t)j;
             if (qi < 1) break;
             uint32_t c3[3];
@@ -1217,6 +1225,7 @@ __device__ __forceinline__ int64_t delta_at(const SharePrep &p, const uint2 *dee
 }
 
 constexpr int kShareWarps = 1;
+constexpr uint32_t kShareLadderBytes = 32u * kDeepLevels * sizeof(uint2);  // a warp's staged ladders
 
 __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     __shared__ LenTables t;
@@ -1225,9 +1234,11 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     // and from DRAM each of its chunks waited out a full load.
     __shared__ __align__(16) float stage[kShareWarps][kMaxSliceCoefs + kMaxSliceCoefs / 32];
     // The ladders of the 32 slices a warp settles, level j of lane l at
-    // [32 j + l]: the settling rounds walk them again and again, and from
-    // global memory every level of the walk was a dependent load.
-    __shared__ uint2 ladders[kShareWarps][32 * kDeepLevels];
+    // [32 j + l] (dynamic shared memory, kShareLadderBytes a warp): the
+    // settling rounds walk them again and again, and from global memory
+    // every level of the walk was a dependent load.
+    extern __shared__ uint2 ladders_all[];
+    uint2 *const ladders = ladders_all + (threadIdx.x >> 5) * (32u * kDeepLevels);
     t.fill();
     __syncthreads();
     const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
@@ -1249,7 +1260,7 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
         const SharePrep mine = next;
         const uint32_t k = k0 + lane;
         const bool live = k < pd.n_slices;
-        uint2 *my_deep = ladders[threadIdx.x >> 5] + lane;
+        uint2 *my_deep = ladders + lane;
         __syncwarp();  // the last chunk's walks are over
         if (live) {
             const uint2 *src = e.deep + (uint64_t)(pd.slice_base + k) * kDeepLevels;
@@ -1739,7 +1750,7 @@ cudaError_t launch_shareout(const EncodeLaunch &e, cudaStream_t s) {
     k_share_prep<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    k_shareout<<<(e.n_pics + kShareWarps - 1) / kShareWarps, 32 * kShareWarps, 0, s>>>(e);
+    k_shareout<<<(e.n_pics + kShareWarps - 1) / kShareWarps, 32 * kShareWarps, kShareWarps * kShareLadderBytes, s>>>(e);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
     k_share_final<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);
     return cudaGetLastError();
@@ -1766,6 +1777,9 @@ cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
 }
 
 cudaError_t configure_encode_kernels() {
+    cudaError_t err0 = cudaFuncSetAttribute(k_shareout, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(kShareWarps * kShareLadderBytes));
+    if (err0 != cudaSuccess) return err0;
     float basis[64];
     dct_basis(basis);
     cudaError_t err = cudaMemcpyToSymbol(c_fdct_basis, basis, sizeof basis);

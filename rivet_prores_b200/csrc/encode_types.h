@@ -17,7 +17,7 @@ constexpr int kWindow = 4;
 // Finer quantisers past the window costed ahead of the share-out for a
 // slice that could reach them (the same prefetch rule, level after level):
 // at most this many per slice; the share-out costs any further one itself.
-constexpr int kDeepLevels = 64;
+constexpr int kDeepLevels = 128;
 // Bytes per frame-header template: 8 + a frame_header() of at most 148.
 constexpr uint32_t kHeaderSlot = 160;
 
