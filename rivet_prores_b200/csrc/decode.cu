@@ -419,6 +419,7 @@ __device__ int decode_alpha(Bits &b, const FrameDesc &fd, const PicDesc &pd, con
     const int32_t mask = (int32_t)((1u << bits) - 1u);
     const uint32_t mag_bits = bits == 8 ? 3u : 6u;
     uint16_t *plane = fd.out_alpha ? fd.out_alpha : alpha + fd.alpha_off;
+    const uint32_t cshift = (uint32_t)__ffs(cols) - 1u;  // cols is 16 times a power of two
     int32_t prev = -1;
     uint32_t n = 0;
     int err;
@@ -426,36 +427,66 @@ __device__ int decode_alpha(Bits &b, const FrameDesc &fd, const PicDesc &pd, con
         if (n >= needed && b.end_of_data()) break;
         uint64_t v;
         int32_t diff;
-        if ((err = b.read(1, v))) return err;
-        if (v == 1) {
-            if ((err = b.read(bits, v))) return err;
-            diff = (int32_t)v;
+        uint32_t run;
+        if (b.remaining() >= 64) {
+            // A difference and a run take at most 34 bits: both from one
+            // look at the next 64, all of them data.
+            const uint64_t w = b.peek();
+            uint32_t used;
+            if (w >> 63) {
+                diff = (int32_t)((w << 1) >> (64u - bits));
+                used = 1u + bits;
+            } else {
+                const int32_t a = (int32_t)((w << 1) >> (64u - mag_bits)) + 1;
+                diff = ((w << (1u + mag_bits)) >> 63) ? -a : a;
+                used = 2u + mag_bits;
+            }
+            const uint64_t u = w << used;
+            if (u >> 63) {
+                run = 1;
+                used += 1u;
+            } else {
+                const uint32_t r4 = (uint32_t)((u << 1) >> 60);
+                if (r4) {
+                    run = r4 + 1u;
+                    used += 5u;
+                } else {
+                    run = (uint32_t)((u << 5) >> 53) + 1u;
+                    used += 16u;
+                }
+            }
+            b.pos += used;
         } else {
-            if ((err = b.read(mag_bits, v))) return err;
-            int32_t a = (int32_t)v + 1;
             if ((err = b.read(1, v))) return err;
-            diff = v ? -a : a;
+            if (v == 1) {
+                if ((err = b.read(bits, v))) return err;
+                diff = (int32_t)v;
+            } else {
+                if ((err = b.read(mag_bits, v))) return err;
+                int32_t a = (int32_t)v + 1;
+                if ((err = b.read(1, v))) return err;
+                diff = v ? -a : a;
+            }
+            if ((err = b.read(1, v))) return err;
+            if (v == 1) {
+                run = 1;
+            } else {
+                if ((err = b.read(4, v))) return err;
+                if (v != 0) {
+                    run = (uint32_t)v + 1;
+                } else {
+                    if ((err = b.read(11, v))) return err;
+                    run = (uint32_t)v + 1;
+                }
+            }
         }
         int32_t value = (int32_t)((uint32_t)prev + (uint32_t)diff) & mask;
         prev = value;
-        uint32_t run;
-        if ((err = b.read(1, v))) return err;
-        if (v == 1) {
-            run = 1;
-        } else {
-            if ((err = b.read(4, v))) return err;
-            if (v != 0) {
-                run = (uint32_t)v + 1;
-            } else {
-                if ((err = b.read(11, v))) return err;
-                run = (uint32_t)v + 1;
-            }
-        }
         if (n + run > count) return DE_ALPHA_RUN;
         uint16_t out = rescale((uint32_t)value, fd.rescale_m, fd.rescale_identity != 0);
         uint32_t stop = min(n + run, needed);
         for (uint32_t i = n; i < stop;) {
-            uint32_t r = i / cols, c = i - r * cols;
+            uint32_t r = i >> cshift, c = i & (cols - 1u);
             uint32_t seg_end = min(stop - i, cols - c);  // samples left in this row of the run
             uint16_t *row = plane + (uint64_t)(pd.first_row + pd.row_step * (16u * sd.mb_y + r)) * width + x0;
             for (uint32_t k = c; k < c + seg_end && k < ncols; k++) row[k] = out;
@@ -640,7 +671,9 @@ constexpr int kEntropyMaxThreads = 512;
 
 // Persistent: each warp takes 32 x entropy_per_lane slice components per
 // grab of the work counter, a lane each in turn, component-major, until the
-// list runs out.
+// list runs out. The alpha components come first: where a frame has alpha,
+// its run/difference codes take a lane several times as long as a colour
+// component, and started last they would leave the launch waiting on them.
 __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) {
     __shared__ uint16_t run_tab[kBookTableWords];
     __shared__ uint16_t level_tab[kBookTableWords];
@@ -661,8 +694,8 @@ __global__ void __launch_bounds__(kEntropyMaxThreads) k_entropy(DecodeLaunch d) 
         for (uint32_t k = 0; k < per_lane; k++) {
             const uint32_t item = base + 32u * k + lane;
             if (item < items) {
-                const uint32_t comp = item / d.n_slices, s = item - comp * d.n_slices;
-                decode_item(d, comp, s, run_tab, level_tab);
+                const uint32_t kind = item / d.n_slices, s = item - kind * d.n_slices;
+                decode_item(d, kind == 0 ? 3u : kind - 1u, s, run_tab, level_tab);
             }
         }
         __syncwarp();

@@ -241,29 +241,37 @@ __device__ uint32_t alpha_runs(const EncodeLaunch &e, const EncSliceDesc &sd, co
     const uint32_t width = fd.width, x0 = 16u * sd.mb_x;
     const uint16_t max_in = (uint16_t)(0xFFFFu >> (16u - fd.bit_depth));
     const uint16_t *plane = e.alpha_in + fd.alpha_in_off;
+    const uint32_t cshift = (uint32_t)__ffs(cols) - 1u;  // cols is 16 times a power of two
     uint32_t n_runs = 0;
     uint32_t prev = 0;
-    for (uint32_t base = 0; base < count; base += 32) {
-        const uint32_t i = base + lane;
-        uint32_t v = 0;
-        if (i < count) {
-            const uint32_t r = i / cols, n = i - r * cols;
+    // 256 values (count is a multiple) a round: their eight loads are all
+    // issued before the first is used.
+    for (uint32_t base = 0; base < count; base += 256) {
+        uint32_t vals[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t i = base + 32u * k + lane;
+            const uint32_t r = i >> cshift, n = i & (cols - 1u);
             const uint32_t row = pd.first_row + pd.row_step * min(16u * sd.mb_y + r, pd.height - 1u);
-            uint32_t a = plane[(uint64_t)row * width + min(x0 + n, width - 1u)];
-            a = a < max_in ? a : max_in;
-            v = fd.rescale_identity ? a : (uint32_t)(((uint64_t)a * fd.rescale_m + (1ull << 39)) >> 40);
+            vals[k] = __ldg(plane + (uint64_t)row * width + min(x0 + n, width - 1u));
         }
-        const uint32_t before = __shfl_up_sync(0xffffffffu, v, 1);
-        const uint32_t left = lane == 0 ? prev : before;
-        const bool is_start = i < count && (i == 0 || v != left);
-        const uint32_t mask = __ballot_sync(0xffffffffu, is_start);
-        if (is_start) {
-            const uint32_t idx = n_runs + __popc(mask & ((1u << lane) - 1u));
-            sc.start[idx] = (uint16_t)i;
-            sc.value[idx] = (uint16_t)v;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t i = base + 32u * k + lane;
+            uint32_t a = vals[k] < max_in ? vals[k] : max_in;
+            const uint32_t v = fd.rescale_identity ? a : (uint32_t)(((uint64_t)a * fd.rescale_m + (1ull << 39)) >> 40);
+            const uint32_t before = __shfl_up_sync(0xffffffffu, v, 1);
+            const uint32_t left = lane == 0 ? prev : before;
+            const bool is_start = i == 0 || v != left;
+            const uint32_t mask = __ballot_sync(0xffffffffu, is_start);
+            if (is_start) {
+                const uint32_t idx = n_runs + __popc(mask & ((1u << lane) - 1u));
+                sc.start[idx] = (uint16_t)i;
+                sc.value[idx] = (uint16_t)v;
+            }
+            n_runs += __popc(mask);
+            prev = __shfl_sync(0xffffffffu, v, 31);
         }
-        n_runs += __popc(mask);
-        prev = __shfl_sync(0xffffffffu, v, 31);
     }
     if (lane == 0) sc.start[n_runs] = (uint16_t)count;
     __syncwarp();
