@@ -968,8 +968,8 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
 // several quantisers of every slice of a picture's tail for nothing. What
 // the ladder leaves out only moves work to the share-out, never changes a
 // size.
-constexpr uint32_t kTailSlices = 64;  // a picture's tail: slices within this many slices' macroblocks of its end
-constexpr uint32_t kTailLevels = 8;
+constexpr uint32_t kTailSlices = 16;  // a picture's tail: slices within this many slices' macroblocks of its end
+constexpr uint32_t kTailLevels = 4;
 
 __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
     __shared__ LenTables t;
@@ -1187,36 +1187,65 @@ __device__ __forceinline__ uint64_t deep_size(const SharePrep &p, uint2 v, bool 
     return (uint64_t)p.hba + (v.x & 0xFFFFu) + (v.x >> 16) + (v.y & 0xFFFFu);
 }
 
-// Steps a slice takes at D through its known levels (the walk of
+// The steps a slice takes at D through its known levels (the walk of
 // src/encode.rs:776-788 while the sizes are known: the window's, then its
-// deep ladder, level j at deep[32 j]), and whether it then needs a level
-// nobody costed (`deep_needed`).
-__device__ __forceinline__ uint32_t steps_at(const SharePrep &p, const uint2 *deep, uint64_t D, int32_t uniform,
-                                             bool &deep_needed) {
-    deep_needed = false;
+// deep ladder, level j at deep[32 j]), as a table the share-out searches
+// each time it settles the slice: at [32 k] the least D that lets the
+// slice take k + 1 steps given that it took k (~0 where the level does not
+// fit), made non-decreasing (a running maximum), so that the steps at D are
+// the number of entries <= D; `len` is where the walk stops whatever D is,
+// and `deep_at_end` whether it then needs a level nobody costed.
+__device__ __forceinline__ void steps_table(const SharePrep &p, const uint2 *deep, int32_t uniform, uint64_t *tab,
+                                            uint32_t &len, bool &deep_at_end) {
+    uint64_t run = 0;
     uint32_t k = 0;
+    deep_at_end = false;
 #pragma unroll
     for (int j = 0; j < kWindow; j++) {
         // k == j steps so far: the quantiser is uniform - j.
-        if (uniform - j <= 1) return k;
-        if (!((p.known >> j) & 1u)) {
-            deep_needed = true;
-            return k;
+        if (uniform - j <= 1) {
+            len = k;
+            return;
         }
-        if (D < p.thr[j]) return k;
+        if (!((p.known >> j) & 1u)) {
+            len = k;
+            deep_at_end = true;
+            return;
+        }
+        run = max(run, p.thr[j]);
+        tab[32u * k] = run;
         k++;
     }
     for (uint32_t j = 0; j < p.deep_count; j++) {
-        if (uniform - (int32_t)k <= 1) return k;
+        if (uniform - (int32_t)k <= 1) {
+            len = k;
+            return;
+        }
         bool fits;
         const uint64_t n = deep_size(p, deep[32u * j], fits);
-        if (!fits) return k;
-        const uint64_t thr = n <= p.base ? 0ull : (((n - p.base) * p.rem) + (1u << p.shift) - 1u) >> p.shift;
-        if (D < thr) return k;
+        const uint64_t thr =
+            !fits ? ~0ull : (n <= p.base ? 0ull : (((n - p.base) * p.rem) + (1u << p.shift) - 1u) >> p.shift);
+        run = max(run, thr);
+        tab[32u * k] = run;
         k++;
     }
-    deep_needed = uniform - (int32_t)k > 1;
-    return k;
+    len = k;
+    deep_at_end = uniform - (int32_t)k > 1;
+}
+
+// The steps at D from steps_table(): a binary search.
+__device__ __forceinline__ uint32_t steps_from(const uint64_t *tab, uint32_t len, bool deep_at_end, uint64_t D,
+                                               bool &deep_needed) {
+    uint32_t lo = 0, hi = len;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tab[32u * mid] <= D)
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    deep_needed = lo == len && deep_at_end;
+    return lo;
 }
 
 // The size over the base after `ks` steps (ks >= 1).
@@ -1233,7 +1262,8 @@ __device__ __forceinline__ int64_t delta_at(const SharePrep &p, const uint2 *dee
 }
 
 constexpr int kShareWarps = 1;
-constexpr uint32_t kShareLadderBytes = 32u * kDeepLevels * sizeof(uint2);  // a warp's staged ladders
+// A warp's staged ladders and steps tables.
+constexpr uint32_t kShareLadderBytes = 32u * kDeepLevels * sizeof(uint2) + 32u * (kWindow + kDeepLevels) * sizeof(uint64_t);
 
 __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     __shared__ LenTables t;
@@ -1247,6 +1277,9 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
     // every level of the walk was a dependent load.
     extern __shared__ uint2 ladders_all[];
     uint2 *const ladders = ladders_all + (threadIdx.x >> 5) * (32u * kDeepLevels);
+    // Each lane's steps_table(), [32 k + lane], after all warps' ladders.
+    uint64_t *const tables = reinterpret_cast<uint64_t *>(ladders_all + kShareWarps * 32u * kDeepLevels) +
+                             (threadIdx.x >> 5) * (32u * (kWindow + kDeepLevels));
     t.fill();
     __syncthreads();
     const uint32_t p = blockIdx.x * kShareWarps + (threadIdx.x >> 5);
@@ -1275,6 +1308,9 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
 #pragma unroll 4
             for (uint32_t j = 0; j < mine.deep_count; j++) my_deep[32u * j] = src[j];
         }
+        uint32_t my_len = 0;
+        bool my_deep_at_end = false;
+        if (live) steps_table(mine, my_deep, st.uniform, tables + lane, my_len, my_deep_at_end);
         __syncwarp();
         // The next chunk's thresholds, fetched while this chunk is walked.
         if (k + 32 < pd.n_slices) next = e.share_prep[pd.slice_base + k + 32];
@@ -1295,7 +1331,7 @@ __global__ void __launch_bounds__(32 * kShareWarps) k_shareout(EncodeLaunch e) {
             uint32_t first_deep = 32;
             for (int round = 0; round < 34; round++) {
                 bool deep = false;
-                ks = live && (uint32_t)lane >= done ? steps_at(mine, my_deep, myD, st.uniform, deep) : 0u;
+                ks = live && (uint32_t)lane >= done ? steps_from(tables + lane, my_len, my_deep_at_end, myD, deep) : 0u;
                 const uint32_t deep_mask = __ballot_sync(0xffffffffu, live && (uint32_t)lane >= done && deep);
                 const uint32_t fd_lane = deep_mask ? (uint32_t)__ffs(deep_mask) - 1u : 32u;
                 const int64_t mine_dl = ks ? delta_at(mine, my_deep, ks) : 0;
