@@ -43,6 +43,11 @@ __device__ __forceinline__ uint32_t floor_clamped(float v, float max) {
     return __float_as_uint(__fadd_rd(c, 8388608.0f)) & 0xFFFFu;
 }
 
+// q exactly, for |q| < 2^22: q added to the significand of 1.5 2^23.
+__device__ __forceinline__ float small_int_to_float(int32_t q) {
+    return __fadd_rn(__int_as_float(0x4B400000 + q), -12582912.0f);
+}
+
 __device__ __forceinline__ uint64_t bswap64(uint64_t v) {
     uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
     return ((uint64_t)__byte_perm(lo, 0, 0x0123) << 32) | __byte_perm(hi, 0, 0x0123);
@@ -772,7 +777,11 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
     // Blocks of a component and its first coefficient in the slice (by
     // select, not an indexed array, which would live in local memory).
     const uint32_t luma_blocks = 4u * mbs, chroma_blocks = cpm * mbs;
+    // Block counts are powers of two: task indices split by shifts, not by
+    // divisions (which run on the conversion pipe this kernel is short of).
+    const uint32_t luma_shift = 31u - __clz(luma_blocks), chroma_shift = 31u - __clz(chroma_blocks);
     const auto blocks_of = [&](uint32_t c) { return c == 0 ? luma_blocks : chroma_blocks; };
+    const auto shift_of = [&](uint32_t c) { return c == 0 ? luma_shift : chroma_shift; };
     const auto start_of = [&](uint32_t c) { return c == 0 ? 0u : 64u * (luma_blocks + (c - 1u) * chroma_blocks); };
     const uint32_t all_blocks = luma_blocks + 2u * chroma_blocks;
     // The row results are held in registers until every thread has read
@@ -789,17 +798,29 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t c = t < luma_blocks * 8u ? 0u : (t < (luma_blocks + chroma_blocks) * 8u ? 1u : 2u);
         const uint32_t tc = t - start_of(c) / 8u;  // 8 row tasks a block
         const uint32_t nb = blocks_of(c);
-        const uint32_t blk = tc % nb, v = tc / nb;
+        const uint32_t blk = tc & (nb - 1u), v = tc >> shift_of(c);
         const int32_t *src = cs + start_of(c);
         const float *sc = scale[c > 0];
         float row[8];
         bool any = false;
+        int32_t q[8];
+        bool wide = false;
 #pragma unroll
         for (int u = 0; u < 8; u++) {
-            const uint32_t kk = 8u * v + u;
-            row[u] = __fmul_rn(__int2float_rn(src[nb * scan[kk] + blk]), sc[kk]);
-            any |= row[u] != 0.0f;
+            q[u] = src[nb * scan[8u * v + u] + blk];
+            wide |= (uint32_t)(q[u] + (1 << 22)) >= (1u << 23);
         }
+        // Values below 2^22 in magnitude convert exactly by an add (no
+        // conversion instruction); a wider one, rare, takes the conversion.
+        if (!wide) {
+#pragma unroll
+            for (int u = 0; u < 8; u++) row[u] = __fmul_rn(small_int_to_float(q[u]), sc[8u * v + u]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 8; u++) row[u] = __fmul_rn(__int2float_rn(q[u]), sc[8u * v + u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) any |= row[u] != 0.0f;
         held_any[k] = any;
         if (any) {
             // Outputs x = 2 j, 2 j + 1 summed as a pair, each in the same
@@ -823,7 +844,7 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t c = t < luma_blocks * 8u ? 0u : (t < (luma_blocks + chroma_blocks) * 8u ? 1u : 2u);
         const uint32_t tc = t - start_of(c) / 8u;  // 8 row tasks a block
         const uint32_t nb = blocks_of(c);
-        const uint32_t blk = tc % nb, v = tc / nb;
+        const uint32_t blk = tc & (nb - 1u), v = tc >> shift_of(c);
         nz[(start_of(c) / 64u + blk) * 8u + v] = held_any[k];
         if (held_any[k]) {
             float *dst = tmp + start_of(c);
@@ -847,7 +868,7 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t c = t < luma_blocks * 4u ? 0u : (t < (luma_blocks + chroma_blocks) * 4u ? 1u : 2u);
         const uint32_t tc = t - start_of(c) / 16u;  // 4 column tasks a block
         const uint32_t nb = blocks_of(c);
-        const uint32_t blk = tc % nb, j = tc / nb;
+        const uint32_t blk = tc & (nb - 1u), j = tc >> shift_of(c);
         const float *src = tmp + start_of(c) + 2u * j * nb + blk;
         const uint64_t rows = *reinterpret_cast<const uint64_t *>(nz + (start_of(c) / 64u + blk) * 8u);
         // Outputs y = 2 i, 2 i + 1 of each column a pair.
@@ -892,7 +913,7 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
         const uint32_t pw = fd.plane_w[c];
         uint16_t *plane = fd.out_planes ? fd.out_planes + (fd.plane_off[c] - fd.plane_off[0]) : d.planes + fd.plane_off[c];
         for (uint32_t t = tid; t < 16u * segs; t += kIdctThreads) {
-            const uint32_t r = t / segs, sx = t - r * segs;
+            const uint32_t r = t >> (31u - __clz(segs)), sx = t & (segs - 1u);
             uint32_t m, bb;
             if (c == 0) {
                 m = sx >> 1;
@@ -976,10 +997,6 @@ struct GroupSlice {
     uint32_t live;        // decoded at all (its picture's slices were located)
 };
 
-// q exactly, for |q| < 2^22: q added to the significand of 1.5 2^23.
-__device__ __forceinline__ float small_int_to_float(int32_t q) {
-    return __fadd_rn(__int_as_float(0x4B400000 + q), -12582912.0f);
-}
 
 
 // One block: dequantise (F = QF scale, src/dsp/scalar.rs:8-12), the IDCT's
