@@ -64,9 +64,9 @@ PUBLISHED_CRATE = ("the crate's README: 1920x1080 422 HQ at 296 encode / 907 dec
 # Figures from ncu captures of these kernels, not measured by this run: the
 # capture's DRAM bytes (read + write) per frame and launch, and issue-slot use.
 CAPTURED = {
-    "k_cost": {"dram_bytes_per_frame": 51.29e6, "issue_active_pct": "39-54",
-               "capture": "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,... on a 14-frame UHD 422 HQ "
-                          "encode, mean of its 9 probe launches"},
+    "k_cost": {"dram_bytes_per_frame": 70.96e6, "issue_active_pct": "41.5",
+               "capture": "ncu --set full on an 8-frame UHD 422 HQ encode, its fifth k_cost launch (a dense probe, "
+                          "which reads every coefficient: the heaviest of the nine)"},
 }
 
 

@@ -84,12 +84,6 @@ __device__ __forceinline__ int32_t quantise1(float f, float inv, float r) {
 
 // ---------------------------------------------------------------- fdct
 
-// v < 2^23 as a float, exactly, by an add: v in the significand of 2^23,
-// less 2^23 (no conversion instruction).
-__device__ __forceinline__ float u16_to_float(uint32_t v) {
-    return __fsub_rn(__uint_as_float(0x4B000000u | v), 8388608.0f);
-}
-
 constexpr int kFdctThreads = 128;
 constexpr int kMaxSliceCoefs = 64 * 12 * 8;
 
@@ -159,14 +153,14 @@ __global__ void __launch_bounds__(kFdctThreads) k_fdct(EncodeLaunch e) {
                 const uint32_t words[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
-                    p[2 * i] = __fsub_rn(__fmul_rn(u16_to_float(words[i] & 0xFFFFu), scale), 256.0f);
-                    p[2 * i + 1] = __fsub_rn(__fmul_rn(u16_to_float(words[i] >> 16), scale), 256.0f);
+                    p[2 * i] = __fsub_rn(__fmul_rn((float)(words[i] & 0xFFFFu), scale), 256.0f);
+                    p[2 * i + 1] = __fsub_rn(__fmul_rn((float)(words[i] >> 16), scale), 256.0f);
                 }
             } else {
 #pragma unroll
                 for (int x = 0; x < 8; x++) {
                     const uint32_t col = min(bx + (uint32_t)x, w - 1u);
-                    p[x] = __fsub_rn(__fmul_rn(u16_to_float(__ldg(line + col)), scale), 256.0f);
+                    p[x] = __fsub_rn(__fmul_rn((float)__ldg(line + col), scale), 256.0f);
                 }
             }
             // Outputs u = 2 j, 2 j + 1 summed as a pair, each in the same
