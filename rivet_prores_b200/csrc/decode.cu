@@ -280,15 +280,31 @@ __device__ __forceinline__ bool window_code(uint32_t t, Codebook cb, uint32_t &s
 // DC by EG5, each next one as a difference by Table 9 on the previous
 // difference, the sign flipped after a negative one.
 template <class Out>
-__device__ int decode_dc(Bits &b, uint32_t n_blocks, Out &out) {
-    uint32_t sym;
-    int err = read_sym(b, nullptr, kFirstDcBook, sym);
-    if (err) return err;
-    int32_t prev_dc = symbol_to_signed(sym);
-    out.put(0, prev_dc);
-    int32_t prev_diff = 3;
-    for (uint32_t i = 1; i < n_blocks; i++) {
-        if ((err = read_sym(b, nullptr, dc_book(prev_diff), sym))) return err;
+__device__ int decode_dc(Bits &b, uint32_t n_blocks, Out &out, Window &win, bool &in_win) {
+    // Each code from the window while 32 or more bits remain (all of them
+    // data, so a codeword of up to 32 bits reads as the general reader
+    // would); otherwise, or for a longer one, the general reader, which
+    // names any failure. The window is left at the first AC code.
+    in_win = b.remaining() >= 32;
+    if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
+    int32_t prev_dc = 0, prev_diff = 3;
+    for (uint32_t i = 0; i < n_blocks; i++) {
+        const Codebook cb = i == 0 ? kFirstDcBook : dc_book(prev_diff);
+        uint32_t sym, len;
+        if (in_win && win.left >= 32u && window_code(win.top(), cb, sym, len)) {
+            win.consume(len);
+        } else {
+            if (in_win) b.pos = b.end - win.left;
+            const int err = read_sym(b, nullptr, cb, sym);
+            if (err) return err;
+            in_win = b.remaining() >= 32;
+            if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
+        }
+        if (i == 0) {
+            prev_dc = symbol_to_signed(sym);
+            out.put(0, prev_dc);
+            continue;
+        }
         int32_t n = symbol_to_signed(sym);
         int32_t diff = prev_diff < 0 ? -n : n;
         int64_t s = (int64_t)prev_dc + diff;
@@ -297,13 +313,16 @@ __device__ int decode_dc(Bits &b, uint32_t n_blocks, Out &out) {
         out.put(i, prev_dc);
         prev_diff = diff;
     }
+    if (in_win) b.pos = b.end - win.left;
     return DE_OK;
 }
 
 template <class Out>
 __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint16_t *run_tab,
                                 const uint16_t *level_tab) {
-    int err = decode_dc(b, n_blocks, out);
+    Window win;
+    bool in_win;
+    int err = decode_dc(b, n_blocks, out, win, in_win);
     if (err) return err;
     const uint32_t total = n_blocks * 64;
     uint32_t n = n_blocks, prev_run = 4, prev_level = 1;
@@ -312,9 +331,6 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
     // reader (which then hands the position back to a fresh window). A lane
     // that takes the general reader leaves the others only for that one
     // iteration.
-    Window win;
-    bool in_win = b.remaining() >= 32;
-    if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
     uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
     for (;;) {
         bool level_next = false;  // the run is read; its level and sign are the general reader's
