@@ -1651,36 +1651,26 @@ __device__ void lane_component_write(BitOut &w, const float *f, const float *cma
 }
 
 // Each slice component's codes, one lane per (component, slice).
-// Persistent like k_cost: each warp takes 32 components (the same one of
-// 32 neighbouring slices) at a time from its own counter.
 __global__ void __launch_bounds__(kCostThreads) k_pack(EncodeLaunch e) {
     __shared__ CodeTables t;
     t.fill_all();
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t items = 3u * e.n_slices;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(e.cost_taken + kProbeSteps, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= items) break;
-        const uint32_t item = base + lane;
-        if (item >= items) continue;
-        const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
-        const EncSliceDesc sd = e.slices[s];
-        const EncPicDesc &pd = e.pics[sd.pic];
-        if (e.frame_status[pd.frame]) continue;
-        const EncFrameDesc &fd = e.frames[pd.frame];
-        const EncPicState &st = e.state[sd.pic];
-        uint64_t at = 8ull * (fd.out_base + st.pic_off + e.slice_off[s] + pd.header_bytes);
-        for (uint32_t c = 0; c < comp; c++) at += 8ull * e.final_comp[3ull * s + c];
-        uint32_t nb, off;
-        comp_layout(fd, sd.mbs, comp, nb, off);
-        BitOut w;
-        w.init(e.out, at);
-        lane_component_write(w, e.coef + sd.coef + off, e.coef_max + ((sd.coef + off) >> 5), nb,
-                             comp_quant(quant_base(e, pd, e.final_qi[s]), comp, nb), t);
-    }
+    const uint32_t item = blockIdx.x * kCostThreads + threadIdx.x;
+    if (item >= 3u * e.n_slices) return;
+    const uint32_t comp = item / e.n_slices, s = item - comp * e.n_slices;
+    const EncSliceDesc sd = e.slices[s];
+    const EncPicDesc &pd = e.pics[sd.pic];
+    if (e.frame_status[pd.frame]) return;
+    const EncFrameDesc &fd = e.frames[pd.frame];
+    const EncPicState &st = e.state[sd.pic];
+    uint64_t at = 8ull * (fd.out_base + st.pic_off + e.slice_off[s] + pd.header_bytes);
+    for (uint32_t c = 0; c < comp; c++) at += 8ull * e.final_comp[3ull * s + c];
+    uint32_t nb, off;
+    comp_layout(fd, sd.mbs, comp, nb, off);
+    BitOut w;
+    w.init(e.out, at);
+    lane_component_write(w, e.coef + sd.coef + off, e.coef_max + ((sd.coef + off) >> 5), nb,
+                         comp_quant(quant_base(e, pd, e.final_qi[s]), comp, nb), t);
 }
 
 // Slice headers and table entries, one thread per slice; alpha codes, one
@@ -1821,14 +1811,7 @@ cudaError_t launch_layout(const EncodeLaunch &e, cudaStream_t s) {
 cudaError_t launch_pack(const EncodeLaunch &e, cudaStream_t s) {
     if (!e.n_slices) return cudaSuccess;
     const uint32_t items = 3u * e.n_slices;
-    static int per_sm = 0;  // resident CTAs of k_pack per SM (the same for every device of a build)
-    if (per_sm == 0) {
-        int fit = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_pack, kCostThreads, 0);
-        per_sm = fit > 0 ? fit : 1;
-    }
-    const uint32_t need = (items + kCostThreads - 1) / kCostThreads;
-    k_pack<<<std::min<uint32_t>(need, (uint32_t)(per_sm * e.sm_count)), kCostThreads, 0, s>>>(e);
+    k_pack<<<(items + kCostThreads - 1) / kCostThreads, kCostThreads, 0, s>>>(e);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
     k_pack_headers<<<(e.n_slices + 255) / 256, 256, 0, s>>>(e);

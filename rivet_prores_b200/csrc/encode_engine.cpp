@@ -331,7 +331,7 @@ static EncodeLaunch encode_params(Context &ctx, Workspace &ws, const EncodePlan 
 static size_t cost_bytes(const EncodePlan &plan) {
     const size_t ns = plan.n_slices + 1;
     return 4 * ns * (1 + 3 * kProbeSteps + 3 * kWindow + 3 + 1) + 8 * ns + sizeof(SharePrep) * ns + 4 * ns + 4 * ns +
-           4 * ns + sizeof(uint2) * kDeepLevels * ns + 4 * kWindow + 4 * (kProbeSteps + 1) + 256;
+           4 * ns + sizeof(uint2) * kDeepLevels * ns + 4 * kWindow + 4 * kProbeSteps + 256;
 }
 
 static Status upload_frames(Workspace &ws, const EncodePlan &plan, const prores_frame *in, cudaStream_t s,
@@ -412,9 +412,6 @@ static Status enqueue_tail(Context &ctx, Workspace &ws, EncodePlan &plan, cudaSt
     PR_CUDA(cudaMemsetAsync(ws.enc_out.p, 0, plan.out_total + 64, s), "memset output");
     PR_CUDA(launch_layout(e, s), "k_layout");
     if ((st = record_kernel(kt, "k_layout", s))) return st;
-    // k_pack's work counter, cleared for every packing pass (a frame that
-    // outgrew its region is packed again).
-    PR_CUDA(cudaMemsetAsync(e.cost_taken + kProbeSteps, 0, sizeof(uint32_t), s), "memset");
     PR_CUDA(launch_pack(e, s), "k_pack");
     if ((st = record_kernel(kt, "k_pack", s))) return st;
     return Status();

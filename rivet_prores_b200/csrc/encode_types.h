@@ -115,7 +115,7 @@ struct EncodeLaunch {
     uint32_t *win_comp;    // [kWindow][slice][3]
     uint32_t *win_list;    // [slice] the slices costed at the current window level
     uint32_t *win_count;   // [kWindow] list lengths
-    uint32_t *cost_taken;  // [kProbeSteps + 1] items the warps of each probe's k_cost, then of k_pack, have taken
+    uint32_t *cost_taken;  // [kProbeSteps] items the warps of each probe's k_cost have taken
     uint32_t *final_comp;  // [slice][3]
     uint32_t *final_qi;    // [slice]
     uint64_t *slice_off;   // [slice] byte offset of the slice in its frame
