@@ -992,23 +992,6 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
         const uint64_t slack = st.budget - st.hi_total;
         const uint64_t most = used + slack * sd.mbs / mbs_from(pd, sd);
         const uint64_t share = slack * sd.mbs / ((uint64_t)pd.width_in_mb * pd.height_in_mb);
-        const uint32_t *c1 = level_comp(e, st, 0, s);
-        uint64_t step = 0;
-        if (c1[0] != kNotCosted) {
-            const uint32_t cc[3] = {c1[0], c1[1], c1[2]};
-            bool f1;
-            const uint64_t n1 = slice_total(hb, cc, alpha, f1);
-            step = n1 > used ? n1 - used : 0u;
-        }
-        // A slice whose first step is small beside its share (a coarse
-        // quantiser, where a step often changes no size) walks many levels
-        // wherever its allowance lands: its ladder goes to the most. So do
-        // the last slices of a picture, where what the slices before left
-        // gathers, for at most kTailLevels levels.
-        const bool coarse = 4u * step <= share;
-        const bool tail = mbs_from(pd, sd) <= (uint64_t)kTailSlices * sd.mbs;
-        const uint64_t likely = coarse || tail ? most : min(most, used + share + share / 4u + step);
-        const uint32_t levels = coarse ? (uint32_t)kDeepLevels : (tail ? kTailLevels : (uint32_t)kDeepLevels);
         const uint32_t *c = level_comp(e, st, kWindow - 1, s);
         bool fits = false;
         uint64_t n = ~0ull;
@@ -1016,6 +999,28 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_deep(EncodeLaunch e) {
             const uint32_t cc[3] = {c[0], c[1], c[2]};
             n = slice_total(hb, cc, alpha, fits);
         }
+        // The slice's step: its size change a finer quantiser, the larger of
+        // the first step and the mean of the window's next three (the first
+        // can be far larger than the rest: above quantiser index 128 a step
+        // of the index is 4 of qScale, below it 1).
+        const uint32_t *c1 = level_comp(e, st, 0, s);
+        uint64_t step = 0, n1 = 0;
+        if (c1[0] != kNotCosted) {
+            const uint32_t cc[3] = {c1[0], c1[1], c1[2]};
+            bool f1;
+            n1 = slice_total(hb, cc, alpha, f1);
+            step = n1 > used ? n1 - used : 0u;
+            if (c[0] != kNotCosted) step = min(step, n > n1 ? (n - n1) / (uint64_t)(kWindow - 1) : 0u);
+        }
+        // A slice whose step is small beside its share (a coarse quantiser,
+        // where a step often changes no size) walks many levels wherever its
+        // allowance lands: its ladder goes to the most. So do the last slices
+        // of a picture, where what the slices before left gathers, for at
+        // most kTailLevels levels.
+        const bool coarse = 4u * step <= share;
+        const bool tail = mbs_from(pd, sd) <= (uint64_t)kTailSlices * sd.mbs;
+        const uint64_t likely = coarse || tail ? most : min(most, used + share + share / 4u + step);
+        const uint32_t levels = coarse ? (uint32_t)kDeepLevels : (tail ? kTailLevels : (uint32_t)kDeepLevels);
         for (uint32_t j = 0; fits && n <= likely && j < levels; j++) {
             const int32_t qi = st.uniform - 1 - kWindow - (int32_t)j;
             if (qi < 1) break;
