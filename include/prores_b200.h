@@ -258,7 +258,7 @@ int prores_encode_device(prores_ctx *ctx, const prores_config *cfg, const prores
 /* Size of the fixed device array prores_decode_noalloc keeps its scratch in.
  * A frame fits when 4 bytes per coefficient position (512 positions per
  * 4:2:2 macroblock, 768 per 4:4:4 one), its frame_size bytes and 64 bytes
- * per slice, plus 21 KiB, come to no more than this: every 1920x1080 frame
+ * per slice, plus 53 KiB, come to no more than this: every 1920x1080 frame
  * whose packet is under about 40 MB (4:4:4) or 50 MB (4:2:2); UHD frames
  * do not fit. */
 #define PRORES_NOALLOC_SCRATCH_BYTES (64u << 20)

@@ -109,22 +109,11 @@ struct Bits {
     }
 };
 
-// One symbol of codebook `cb` (src/vlc.rs:207-230), with a prefix-table
-// shortcut for codewords of 9 bits or fewer that lie wholly inside the data
-// (those decode the same either way; anything else takes the general path,
-// which also names the failure exactly as the crate does).
-__device__ __forceinline__ int read_sym(Bits &b, const uint16_t *tab, Codebook cb, uint32_t &sym) {
+// One symbol of codebook `cb` (src/vlc.rs:207-230), read bit by bit as the
+// crate reads it, naming any failure exactly as the crate does.
+__device__ __forceinline__ int read_sym(Bits &b, Codebook cb, uint32_t &sym) {
     uint64_t w = b.peek();
     uint64_t rem = b.remaining();
-    if (tab) {
-        uint32_t e = tab[w >> (64 - kDecodeBits)];
-        uint32_t l = e & 31;
-        if (e && l <= rem) {
-            sym = e >> 5;
-            b.pos += l;
-            return DE_OK;
-        }
-    }
     uint32_t lz = clz64(w);
     if (lz > kMaxPrefix) return DE_PREFIX;
     if ((uint64_t)lz >= rem) return DE_PAST_END;
@@ -295,7 +284,7 @@ __device__ int decode_dc(Bits &b, uint32_t n_blocks, Out &out, Window &win, bool
             win.consume(len);
         } else {
             if (in_win) b.pos = b.end - win.left;
-            const int err = read_sym(b, nullptr, cb, sym);
+            const int err = read_sym(b, cb, sym);
             if (err) return err;
             in_win = b.remaining() >= 32;
             if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
@@ -331,19 +320,19 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
     // reader (which then hands the position back to a fresh window). A lane
     // that takes the general reader leaves the others only for that one
     // iteration.
-    uint32_t rrow = run_book_row(prev_run) * kDecodeEntries, lrow = level_book_row(prev_level) * kDecodeEntries;
+    uint32_t rrow = run_book_row(prev_run) * kBookEntries, lrow = level_book_row(prev_level) * kBookEntries;
     for (;;) {
         bool level_next = false;  // the run is read; its level and sign are the general reader's
         if (in_win && win.left >= 32u) {
             const uint32_t t = win.top();
-            const uint32_t e1 = run_tab[rrow + (t >> (32 - kDecodeBits))];
+            const uint32_t e1 = run_tab[rrow + (t >> (32 - kBookBits))];
             uint32_t run = 0, l = 0;
             bool got = true;
             if (e1) {
                 l = e1 & 15u;
                 run = (e1 >> 4) & 63u;
                 const uint32_t t2 = t << l;
-                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kDecodeBits))];
+                const uint32_t e2 = level_tab[lrow + (t2 >> (32 - kBookBits))];
                 if (e2) {
                     // Run, level and sign in one go.
                     const uint32_t l2 = e2 & 15u;
@@ -354,8 +343,8 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
                     const int32_t level = (int32_t)prev_level + 1;
                     out.put(n, (t2 << l2) >> 31 ? -level : level);
                     n += 1;
-                    rrow = (e1 >> 10) * kDecodeEntries;
-                    lrow = (e2 >> 10) * kDecodeEntries;
+                    rrow = (e1 >> 10) * kBookEntries;
+                    lrow = (e2 >> 10) * kBookEntries;
                     win.consume(l + l2 + 1u);
                     continue;
                 }
@@ -371,7 +360,7 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
                 got = false;
                 if (win.left >= 32u) {
                     const uint32_t u = win.top();
-                    const uint32_t e2 = level_tab[lrow + (u >> (32 - kDecodeBits))];
+                    const uint32_t e2 = level_tab[lrow + (u >> (32 - kBookBits))];
                     if (e2) {
                         lvl = (e2 >> 4) & 63u;
                         l = e2 & 15u;
@@ -389,8 +378,8 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
                     const int32_t level = (int32_t)lvl + 1;
                     out.put(n, neg ? -level : level);
                     n += 1;
-                    rrow = run_book_row(prev_run) * kDecodeEntries;
-                    lrow = level_book_row(prev_level) * kDecodeEntries;
+                    rrow = run_book_row(prev_run) * kBookEntries;
+                    lrow = level_book_row(prev_level) * kBookEntries;
                     continue;
                 }
                 level_next = true;
@@ -401,13 +390,13 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
         if (!level_next) {
             if (b.remaining() <= 31 && b.peek() == 0) break;  // endOfData()
             uint32_t run;
-            if ((err = read_sym(b, nullptr, run_book(prev_run), run))) return err;
+            if ((err = read_sym(b, run_book(prev_run), run))) return err;
             prev_run = run;
             n += run;
             if (n >= total) return DE_RUN_PAST_END;
         }
         uint32_t lvl;
-        if ((err = read_sym(b, nullptr, level_book(prev_level), lvl))) return err;
+        if ((err = read_sym(b, level_book(prev_level), lvl))) return err;
         prev_level = lvl;
         if (b.remaining() < 1) return DE_PAST_END;
         const bool neg = b.peek() >> 63;
@@ -415,8 +404,8 @@ __device__ int decode_component(Bits &b, uint32_t n_blocks, Out &out, const uint
         const int32_t level = (int32_t)lvl + 1;
         out.put(n, neg ? -level : level);
         n += 1;
-        rrow = run_book_row(prev_run) * kDecodeEntries;
-        lrow = level_book_row(prev_level) * kDecodeEntries;
+        rrow = run_book_row(prev_run) * kBookEntries;
+        lrow = level_book_row(prev_level) * kBookEntries;
         in_win = b.remaining() >= 32;
         if (in_win) win.init(reinterpret_cast<const uint8_t *>(b.w), b.pos, b.end);
     }
@@ -984,7 +973,6 @@ __global__ void __launch_bounds__(kIdctThreads, 5) k_idct(DecodeLaunch d) {
 
 constexpr int kDecodeThreads = 128;
 constexpr uint32_t kMaxGroup = 32;  // slices a CTA decodes at once (4 items each <= 128 threads)
-constexpr uint32_t kBookEntries = 6 * kDecodeEntries;  // one prefix-table row per distinct codebook
 
 // Figures 4 and 5, folded into immediates in the unrolled transform:
 // scan_at<IL>(8 v + u) is the scanned index of row v, column u.
@@ -1076,13 +1064,13 @@ template <class T>
 __global__ void __launch_bounds__(kDecodeThreads) k_decode(DecodeLaunch d) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint16_t *run_tab = reinterpret_cast<uint16_t *>(smem);
-    uint16_t *level_tab = run_tab + kBookEntries;
-    GroupSlice *gs = reinterpret_cast<GroupSlice *>(level_tab + kBookEntries);  // kMaxGroup
+    uint16_t *level_tab = run_tab + kBookTableWords;
+    GroupSlice *gs = reinterpret_cast<GroupSlice *>(level_tab + kBookTableWords);  // kMaxGroup
     float *scale = reinterpret_cast<float *>(gs + kMaxGroup);                    // [group][luma, chroma][64]
     T *slots = reinterpret_cast<T *>(scale + 128u * d.group);                   // group_positions
     __shared__ uint32_t s_group, s_blocks;
 
-    for (uint32_t i = threadIdx.x; i < kBookEntries / 2; i += kDecodeThreads) {
+    for (uint32_t i = threadIdx.x; i < kBookTableWords / 2; i += kDecodeThreads) {
         reinterpret_cast<uint32_t *>(run_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.run_books)[i];
         reinterpret_cast<uint32_t *>(level_tab)[i] = reinterpret_cast<const uint32_t *>(d.tables.level_books)[i];
     }
@@ -1279,7 +1267,7 @@ cudaError_t launch_status(const DecodeLaunch &d, cudaStream_t s) {
 }
 
 size_t decode_smem_bytes(uint32_t group, uint32_t group_positions, uint32_t slot_bytes) {
-    return 2 * 2 * kBookEntries + sizeof(GroupSlice) * kMaxGroup + 512u * group + slot_bytes * group_positions;
+    return 2 * 2 * kBookTableWords + sizeof(GroupSlice) * kMaxGroup + 512u * group + slot_bytes * group_positions;
 }
 
 // The most shared memory a CTA of k_decode may take (a group of 8-macroblock

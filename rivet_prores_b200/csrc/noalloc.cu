@@ -38,7 +38,8 @@ namespace {
 static __device__ __align__(256) unsigned char g_scratch[PRORES_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-constexpr size_t kTablesBytes = 16 << 10;  // the run and level prefix tables (a row per codebook)
+constexpr size_t kTablesBytes = 2 * 2 * kBookTableWords;  // the run and level prefix tables (a row per codebook)
+static_assert(kTablesBytes % 256 == 0, "the descriptors after the tables stay 256-byte aligned");
 constexpr size_t kDescBytes = 4 << 10;     // frame and picture descriptors, statuses, weights, counter
 
 struct DeviceSetup {
