@@ -196,16 +196,19 @@ __device__ __forceinline__ void list_entry(const uint32_t *w, uint32_t cap, uint
 
 // The read position as a 64-bit window consumed from the top: `cur` holds
 // the bits [pos, pos + avail) MSB first with zeros below, and is refilled
-// 32 bits at a time from big-endian words fetched one word ahead, so that a
-// symbol costs shifts of the window rather than a fresh funnel shift of two
-// words. Reads the same bits as Bits; only used while at least 32 bits of
-// the component remain, so the top 32 bits are always data.
+// 32 bits at a time from the words after it, which are fetched two ahead
+// and kept as loaded (byte-swapped only when they enter the window), so a
+// refill never waits for the load it issues. A symbol costs shifts of the
+// window rather than a fresh funnel shift of two words. Reads the same
+// bits as Bits; only used while at least 32 bits of the component remain,
+// so the top 32 bits are always data. The words fetched reach 12 bytes past
+// the component's data at most, inside the bitstream buffer's padding.
 struct Window {
     const uint32_t *w;
     uint64_t cur;
     uint32_t avail, left;  // valid bits in cur (>= 32); bits of the component from pos on
     uint64_t next;         // index of the word after those in cur
-    uint32_t nxt;          // that word
+    uint32_t raw1, raw2;   // words next and next + 1, as loaded
 
     __device__ __forceinline__ static uint32_t be32(uint32_t v) { return __byte_perm(v, 0, 0x0123); }
     __device__ __forceinline__ void init(const uint8_t *base, uint64_t pos, uint64_t end) {
@@ -215,7 +218,8 @@ struct Window {
         cur = (((uint64_t)be32(__ldg(w + i)) << 32) | be32(__ldg(w + i + 1))) << skip;
         avail = 64u - skip;
         next = i + 2;
-        nxt = be32(__ldg(w + next));
+        raw1 = __ldg(w + next);
+        raw2 = __ldg(w + next + 1);
         left = (uint32_t)(end - pos);
     }
     __device__ __forceinline__ uint32_t top() const { return (uint32_t)(cur >> 32); }
@@ -224,9 +228,10 @@ struct Window {
         avail -= len;
         left -= len;
         if (avail < 32u) {
-            cur |= (uint64_t)nxt << (32u - avail);
+            cur |= (uint64_t)be32(raw1) << (32u - avail);
             avail += 32u;
-            nxt = be32(__ldg(w + ++next));
+            raw1 = raw2;
+            raw2 = __ldg(w + ++next + 1);
         }
     }
 };
