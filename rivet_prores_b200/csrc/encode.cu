@@ -958,15 +958,17 @@ __global__ void __launch_bounds__(kCostThreads) k_cost_window(EncodeLaunch e, in
 //
 // The likely allowance is the slice's share of the picture's slack in
 // proportion to its macroblocks, plus a quarter, plus one step (its size
-// change at the first finer quantiser), and never above the most its share
-// can come to (the crate's prefetch rule: the whole slack from the slice on,
-// if no slice before it took any); for a slice whose step is under a
-// quarter of its share, it is that most. The share-out's allowance for a slice is
-// what the slices before it left, which stays near the proportional share
-// but for the last few slices of a picture; the most is far above it there
-// (the last slice's is the whole slack), and a ladder to the most costed
-// several quantisers of every slice of a picture's tail for nothing. What
-// the ladder leaves out only moves work to the share-out, never changes a
+// change a finer quantiser, as estimated below), and never above the most
+// its share can come to (the crate's prefetch rule: the whole slack from
+// the slice on, if no slice before it took any). For a slice whose step is
+// under a quarter of its share it is that most, and so it is, for at most
+// kTailLevels levels, for a picture's last kTailSlices slices. The
+// share-out's allowance for a slice is what the slices before it left,
+// which stays near the proportional share but for the last slices of a
+// picture; the most is far above it there (the last slice's is the whole
+// slack), and a ladder to the most for every slice costed several
+// quantisers of every slice of a picture's tail for nothing. What the
+// ladder leaves out only moves work to the share-out, never changes a
 // size.
 constexpr uint32_t kTailSlices = 16;  // a picture's tail: slices within this many slices' macroblocks of its end
 constexpr uint32_t kTailLevels = 4;
