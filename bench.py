@@ -68,6 +68,19 @@ CAPTURED = {
                "capture": "ncu --set full on an 8-frame UHD 422 HQ encode, its fifth k_cost launch (a dense probe, "
                           "which reads every coefficient: the heaviest of the nine)"},
 }
+# What limits each kernel, from the ncu captures summarised under profiles/.
+# The roofline's "bound" is the roof the kernel is measured against (HBM
+# bandwidth: the work is byte and integer work, no tensor-core math); none of
+# these kernels reaches it, and "limiter" names what holds it back instead.
+LIMITER = {
+    "k_cost": "latency: 41.5 % of issue slots active, a quarter to two fifths of the warp slots busy",
+    "k_cost_window": "latency, as k_cost",
+    "k_fdct": "instruction issue (83 % of issue slots active)",
+    "k_pack": "latency: half of each warp's lanes active",
+    "k_entropy": "latency: a warp waits for its longest component",
+    "k_idct": "instruction issue (about 108 instructions per sample)",
+    "k_decode": "latency: too few components in flight per SM for the entropy step",
+}
 
 
 def parse_args():
@@ -451,7 +464,7 @@ def run_b200(args):
     p_frame = pkt_bytes / B
     kernels = {}
     for name, ms in sorted(kernel_ms.items(), key=lambda x: -x[1]):
-        entry = {"ms_per_step": round(ms, 4), "launches": counts[name]}
+        entry = {"ms_per_step": round(ms, 4), "launches": counts[name], "limiter": LIMITER.get(name)}
         if name in KERNEL_BYTES:
             fn, basis = KERNEL_BYTES[name]
             per_launch = fn(SAMPLES, p_frame) * B
@@ -465,7 +478,8 @@ def run_b200(args):
     step_gbs = step_bytes / (ms_per_step / 1000.0) / 1e9
     cap = CAPTURED.get(dominant)
     roofline = {
-        "kernel": dominant, "bound": "hbm", "achieved": dom.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
+        "kernel": dominant, "bound": "hbm", "limiter": LIMITER.get(dominant),
+        "achieved": dom.get("achieved_gbs"), "peak": peak, "unit": "GB/s",
         "frac": dom.get("frac"), "peak_source": f"{peak_kind} (HBM copy bandwidth)",
         "algorithmic_bytes_per_launch": dom.get("algorithmic_bytes_per_launch"), "basis": dom.get("basis"),
         "launch_ms": round(kernel_ms[dominant] / counts[dominant], 4), "launches_per_step": counts[dominant],
