@@ -102,6 +102,12 @@ cudaError_t DeviceBuf::reserve(size_t bytes) {
     p = nullptr;
     cap = 0;
     cudaError_t e = cudaMallocAsync(&p, want, stream);
+    if (e == cudaErrorMemoryAllocation && owner) {
+        // Idle workspaces may hold what this growth needs.
+        cudaGetLastError();
+        owner->trim(0);
+        e = cudaMallocAsync(&p, want, stream);
+    }
     // Usable from any stream once the workspace's stream has passed it.
     if (e == cudaSuccess) {
         cudaEvent_t ev;
@@ -230,13 +236,24 @@ cudaError_t Stager::finish() {
     return cudaSuccess;
 }
 
-void Workspace::bind_stream() {
+void Workspace::bind_stream(Context *owner) {
     for (DeviceBuf *b : {&bits, &frames, &pics, &slices, &slot_status, &pic_status, &coef, &coef_count, &planes,
                          &alpha, &weights, &counter, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost, &enc_pic_state,
                          &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes, &enc_frame_out}) {
         b->stream = stream;
         b->wait_ms = wait_ms;
+        b->owner = owner;
     }
+}
+
+size_t Workspace::device_bytes() const {
+    size_t n = 0;
+    for (const DeviceBuf *b : {&bits, &frames, &pics, &slices, &slot_status, &pic_status, &coef, &coef_count, &planes,
+                               &alpha, &weights, &counter, &enc_in, &enc_alpha_in, &enc_coef, &enc_cost,
+                               &enc_pic_state, &enc_out, &enc_slice_out, &enc_alpha_bits, &enc_alpha_bytes,
+                               &enc_frame_out})
+        n += b->cap;
+    return n;
 }
 
 Workspace::~Workspace() {
@@ -263,7 +280,7 @@ std::unique_ptr<Workspace> Context::acquire() {
             auto ws = std::move(free_ws.back());
             free_ws.pop_back();
             ws->wait_ms = ws->stager.wait_ms = limit;
-            ws->bind_stream();
+            ws->bind_stream(this);
             return ws;
         }
     }
@@ -272,15 +289,41 @@ std::unique_ptr<Workspace> Context::acquire() {
     ws->wait_ms = ws->stager.wait_ms = limit;
     cudaSetDevice(device);
     if (cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
-    ws->bind_stream();
+    ws->bind_stream(this);
     return ws;
 }
 
 void Context::release(std::unique_ptr<Workspace> ws) {
     if (!ws) return;
     ws->stager.forget();
-    std::lock_guard<std::mutex> g(m);
-    free_ws.push_back(std::move(ws));
+    size_t held = 0;
+    {
+        std::lock_guard<std::mutex> g(m);
+        free_ws.push_back(std::move(ws));
+        for (const auto &w : free_ws) held += w->device_bytes();
+    }
+    if (held > keep_free_bytes) trim(keep_free_bytes);
+}
+
+void Context::trim(size_t keep) {
+    std::vector<std::unique_ptr<Workspace>> drop;
+    {
+        std::lock_guard<std::mutex> g(m);
+        std::sort(free_ws.begin(), free_ws.end(),
+                  [](const std::unique_ptr<Workspace> &a, const std::unique_ptr<Workspace> &b) {
+                      return a->device_bytes() < b->device_bytes();
+                  });
+        size_t held = 0;
+        for (const auto &w : free_ws) held += w->device_bytes();
+        while (held > keep && !free_ws.empty()) {
+            held -= free_ws.back()->device_bytes();
+            drop.push_back(std::move(free_ws.back()));
+            free_ws.pop_back();
+        }
+    }
+    // Freed outside the lock: each cudaFree waits for the device.
+    cudaSetDevice(device);
+    drop.clear();
 }
 
 void Context::refresh(Workspace &ws) {
@@ -290,7 +333,7 @@ void Context::refresh(Workspace &ws) {
         limit = wait_ms;
     }
     ws.wait_ms = ws.stager.wait_ms = limit;
-    ws.bind_stream();
+    ws.bind_stream(this);
 }
 
 void Context::release_or_retire(std::unique_ptr<Workspace> ws, cudaGraphExec_t graph) {
@@ -777,6 +820,9 @@ prores_ctx *prores_create(int device) {
         uint64_t keep = 8ull << 30;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    // Idle workspaces keep their buffers for the next call, up to a quarter
+    // of the device's memory; past that the largest are freed.
+    ctx->impl.keep_free_bytes = prop.totalGlobalMem / 4;
     ctx->impl.entropy = EntropyShape{ctx->impl.tuning.entropy_warps_per_block,
                                      entropy_grid(device, ctx->impl.tuning.entropy_warps_per_block,
                                                   ctx->impl.tuning.entropy_blocks_per_sm)};

@@ -21,11 +21,16 @@ namespace prores {
 // its workspace's stream (set when the workspace is made), and the growth
 // waits for that stream only: cudaFree and cudaMalloc would wait for the
 // whole device, which stalls every other thread's batch.
+struct Context;
+
 struct DeviceBuf {
     void *p = nullptr;
     size_t cap = 0;
     cudaStream_t stream = nullptr;
     uint32_t wait_ms = 0;  // bound on the wait for a growth (0: none)
+    // The context whose idle workspaces are freed when a growth finds the
+    // device out of memory (then the growth is tried once more).
+    Context *owner = nullptr;
     cudaError_t reserve(size_t bytes);
     template <class T>
     T *as() const {
@@ -94,8 +99,10 @@ struct Workspace {
     DeviceBuf enc_in, enc_alpha_in, enc_coef, enc_cost, enc_pic_state, enc_out, enc_slice_out, enc_alpha_bits,
         enc_alpha_bytes, enc_frame_out;
     PinnedBuf host_stage;
-    // Points every DeviceBuf at the workspace's stream.
-    void bind_stream();
+    // Points every DeviceBuf at the workspace's stream and at `owner`.
+    void bind_stream(Context *owner);
+    // Device bytes its buffers hold.
+    size_t device_bytes() const;
     // Statuses and sizes read back each call. Pinned, because a copy into
     // pageable memory returns only when done and keeps other host threads'
     // CUDA calls waiting meanwhile.
@@ -136,7 +143,13 @@ struct Context {
     uint32_t wait_ms = kDefaultWaitMs;
     Tuning current_tuning();
     EntropyShape current_entropy();
+    // Idle workspaces, kept with their buffers for the next call; at most
+    // keep_free_bytes of device memory stays in them (the largest go first).
     std::vector<std::unique_ptr<Workspace>> free_ws;
+    size_t keep_free_bytes = 0;
+    // Frees idle workspaces, the largest first, until they hold at most
+    // `keep` device bytes.
+    void trim(size_t keep);
     // Workspaces whose stream still had work when a wait ran out or their
     // call gave up: reused once that work is done, never before.
     struct Retired {
