@@ -48,7 +48,6 @@ TARGET = 3_643_238  # Profile::target_frame_bytes(HQ, 3840, 2160)
 KERNEL_BYTES = {
     "k_fdct": (lambda s, p: 2 * s + 4 * s + s // 8, "planes in (2 B a sample), f32 coefficients and chunk maxima out"),
     "k_cost": (lambda s, p: 4 * s + s // 8, "f32 coefficients and chunk maxima a probe reads when it skips no chunk"),
-    "k_cost_window": (lambda s, p: 4 * s + s // 8, "f32 coefficients and chunk maxima, every slice costed"),
     "k_pack": (lambda s, p: 4 * s + s // 8 + p, "f32 coefficients and chunk maxima in, packet out"),
     "k_decode": (lambda s, p: p + 2 * s, "packet in, u16 planes out"),
     "k_entropy": (lambda s, p: p, "packet in (coefficient lists are an intermediate)"),
@@ -74,7 +73,8 @@ CAPTURED = {
 # these kernels reaches it, and "limiter" names what holds it back instead.
 LIMITER = {
     "k_cost": "latency: 41.5 % of issue slots active, a quarter to two fifths of the warp slots busy",
-    "k_cost_window": "latency, as k_cost",
+    "k_cost_window": "latency, as k_cost; it costs a list of slices that changes with the pictures (level 0 "
+                     "copies from a probe at the same quantiser where there is one), so it has no fixed byte basis",
     "k_fdct": "instruction issue (83 % of issue slots active)",
     "k_pack": "latency: half of each warp's lanes active",
     "k_entropy": "latency: a warp waits for its longest component",
@@ -88,7 +88,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--unique", type=int, default=0, help="distinct pictures in a batch (0: all of them)")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
@@ -403,8 +403,7 @@ def run_b200(args):
     if not args.no_tune:
         from rivet_prores_b200 import autotune
 
-        autotune.tune(device=local, quick=True, store=False, frames=frames, stage_frames=frames,
-                      depths=[2, 3, 4, 6, 8])
+        autotune.tune(device=local, quick=True, store=False, frames=frames, stage_frames=frames)
         tuning_note = "tuned in this run (rivet_prores_b200.autotune, quick search)"
     from dataclasses import asdict
 
