@@ -110,7 +110,10 @@ typedef struct prores_frame_header {
 
 /* A context on CUDA device `device`; NULL on failure (no device, or not
  * sm_100). Replaces constructing Decoder/Encoder values: the crate's are
- * stateless settings holders, this one owns device workspaces. */
+ * stateless settings holders, this one owns device workspaces. A finished
+ * call's workspace stays with the context, buffers and all, for the next
+ * call; idle ones keep at most a quarter of the device's memory, and are
+ * all freed when a call's allocation would otherwise fail. */
 prores_ctx *prores_create(int device);
 void prores_destroy(prores_ctx *ctx);
 
