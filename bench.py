@@ -64,6 +64,7 @@ PUBLISHED_CRATE = ("the crate's README: 1920x1080 422 HQ at 296 encode / 907 dec
 # capture's DRAM bytes (read + write) per frame and launch, and issue-slot use.
 CAPTURED = {
     "k_cost": {"dram_bytes_per_frame": 70.96e6, "issue_active_pct": "41.5",
+               "thread_instructions_per_coefficient": 26.7,
                "capture": "ncu --set full on an 8-frame UHD 422 HQ encode, its fifth k_cost launch (a dense probe, "
                           "which reads every coefficient: the heaviest of the nine)"},
 }
@@ -487,6 +488,7 @@ def run_b200(args):
         "traffic_source": (cap["capture"] + ", scaled to this launch's frames; not measured by this run")
         if cap else "no capture of this kernel",
         "issue_active_pct": cap["issue_active_pct"] if cap else None,
+        "thread_instructions_per_coefficient": cap.get("thread_instructions_per_coefficient") if cap else None,
         "step": {"bytes": int(step_bytes), "basis": "packet + u16 planes, each direction, every frame",
                  "ms": round(ms_per_step, 4), "achieved_gbs": round(step_gbs, 2),
                  "frac": round(step_gbs / peak, 4)},
