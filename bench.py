@@ -55,9 +55,10 @@ KERNEL_BYTES = {
 }
 # What the CPU codec timed beside the GPU is, and what the crate itself
 # publishes for the same work on other hardware.
-CPU_CODE = ("the oracle's scalar restatement of the crate's CPU path, with its slice-parallel pool (no hand-written "
-            "SIMD; the crate's SIMD levels give bit-identical output, so this is a slower, equal-output stand-in), "
-            "compiled -O3 -march=x86-64-v3 -ffp-contract=off")
+CPU_CODE = ("the oracle's restatement of the crate's CPU path, with its slice-parallel pool and AVX2 forms of the dsp "
+            "kernels (IDCT, FDCT, quantise), which give the scalar forms' results bit for bit as the crate's own SIMD "
+            "levels do; entropy coding and rate control scalar, as in the crate; compiled -O3 -march=x86-64-v3 "
+            "-ffp-contract=off")
 PUBLISHED_CRATE = ("the crate's README: 1920x1080 422 HQ at 296 encode / 907 decode frames/s on 32 threads of a Ryzen 9 "
                    "9950X, about 74 / 227 at UHD (4x the samples), about 56 round trips/s; other hardware")
 # Figures from ncu captures of these kernels, not measured by this run: the

@@ -100,6 +100,7 @@ def lib():
         L.ora_basis.argtypes = [P(ctypes.c_float)]
         L.ora_idct_put.argtypes = [P(ctypes.c_int32), P(ctypes.c_float), ctypes.c_uint32, P(ctypes.c_uint16)]
         L.ora_fdct_load.argtypes = [P(ctypes.c_uint16), ctypes.c_float, P(ctypes.c_float)]
+        L.ora_set_simd.argtypes = [ctypes.c_int]
         L.ora_quantise.argtypes = [P(ctypes.c_float), ctypes.c_size_t, P(ctypes.c_float), ctypes.c_float,
                                    P(ctypes.c_int32), P(ctypes.c_uint64)]
         L.ora_encode_coefficients.argtypes = [P(ctypes.c_int32), ctypes.c_size_t, P(ctypes.c_uint8),
@@ -307,6 +308,12 @@ def basis() -> np.ndarray:
     b = np.zeros(64, np.float32)
     lib().ora_basis(_ptr(b, ctypes.c_float))
     return b
+
+
+def set_simd(on: bool) -> None:
+    """Runs the dsp kernels (IDCT, FDCT, quantise) in their AVX2 forms (the
+    default) or their scalar forms, process-wide; both give the same results."""
+    lib().ora_set_simd(1 if on else 0)
 
 
 def idct_put(coef: np.ndarray, scale: np.ndarray, depth: int) -> np.ndarray:

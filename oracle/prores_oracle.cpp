@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <immintrin.h>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -557,7 +558,7 @@ inline uint16_t sat_u16(float x) {
 }
 
 // src/dsp/scalar.rs:8-12
-void idct_put(const int32_t coef[64], const float scale[64], Output o, uint16_t out[64]) {
+void idct_put_scalar(const int32_t coef[64], const float scale[64], Output o, uint16_t out[64]) {
     float f[64], v[64];
     for (int k = 0; k < 64; k++) f[k] = (float)coef[k] * scale[k];
     idct(f, v);
@@ -569,15 +570,15 @@ void idct_put(const int32_t coef[64], const float scale[64], Output o, uint16_t 
 }
 
 // src/dsp/scalar.rs:14-17
-void fdct_load(const uint16_t pix[64], float scale, float out[64]) {
+void fdct_load_scalar(const uint16_t pix[64], float scale, float out[64]) {
     float p[64];
     for (int k = 0; k < 64; k++) p[k] = (float)pix[k] * scale - 256.0f;
     fdct(p, out);
 }
 
 // src/dsp/scalar.rs:19-39
-void quantise(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out,
-              uint64_t *mask) {
+void quantise_scalar(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out,
+                     uint64_t *mask) {
     for (size_t i = 0; i < n; i++) mask[i] = 0;
     for (size_t s = 0; s < 64; s++) {
         float r = s == 0 ? 0.5f : ac_rounding;
@@ -591,6 +592,137 @@ void quantise(const float *f, size_t n, const float inv[64], float ac_rounding, 
             mask[i / 64] |= (uint64_t)(q != 0) << (i % 64);
         }
     }
+}
+
+// ---------------------------------------------------------------- dsp, AVX2
+// The crate dispatches its dsp kernels to SIMD forms that give the scalar
+// forms' results bit for bit (src/dsp/mod.rs:1-20, :102-178). These are
+// this oracle's own 8-wide forms of the three scalar kernels above: every
+// lane does the scalar kernel's multiplies and adds in the same order, one
+// rounding each (-ffp-contract=off keeps the intrinsics unfused), so each
+// output equals the scalar one. They make the timed CPU baseline closer to
+// the crate's speed; `ora_set_simd(0)` runs the scalar forms instead, and
+// the tests check that both give the same bytes and samples.
+std::atomic<bool> g_simd{true};
+
+// The basis transposed, tt[8 u + x] = t[8 x + u]: the row of products a
+// coefficient u contributes to the eight outputs x.
+struct BasisT {
+    alignas(32) float tt[64];
+    BasisT() {
+        const float *t = basis().t;
+        for (int x = 0; x < 8; x++)
+            for (int u = 0; u < 8; u++) tt[8 * u + x] = t[8 * x + u];
+    }
+};
+const BasisT &basis_t() {
+    static BasisT b;
+    return b;
+}
+
+// idct_put_scalar, eight outputs at a time.
+void idct_put_avx2(const int32_t coef[64], const float scale[64], Output o, uint16_t out[64]) {
+    const float *t = basis().t, *tt = basis_t().tt;
+    alignas(32) float f[64];
+    for (int v = 0; v < 8; v++)
+        _mm256_store_ps(f + 8 * v, _mm256_mul_ps(_mm256_cvtepi32_ps(_mm256_loadu_si256(
+                                                      reinterpret_cast<const __m256i *>(coef + 8 * v))),
+                                                  _mm256_loadu_ps(scale + 8 * v)));
+    // Rows: tmp[v][x] = 0 + row[0] T[x][0] + ... + row[7] T[x][7]; an
+    // all-zero row (-0 counts as zero) stays zero.
+    const __m256 zero = _mm256_setzero_ps();
+    __m256 tmp[8];
+    for (int v = 0; v < 8; v++) {
+        const __m256 row = _mm256_load_ps(f + 8 * v);
+        tmp[v] = zero;
+        if (_mm256_movemask_ps(_mm256_cmp_ps(row, zero, _CMP_EQ_OQ)) == 0xFF) continue;
+        __m256 acc = zero;
+        for (int u = 0; u < 8; u++)
+            acc = _mm256_add_ps(acc, _mm256_mul_ps(_mm256_broadcast_ss(f + 8 * v + u), _mm256_load_ps(tt + 8 * u)));
+        tmp[v] = acc;
+    }
+    // Columns: out[y][x] = 0 + T[y][0] tmp[0][x] + ... + T[y][7] tmp[7][x],
+    // then floor(v scale + bias) clamped to [0, max].
+    const __m256 sc = _mm256_set1_ps(o.scale), bias = _mm256_set1_ps(o.bias), mx = _mm256_set1_ps(o.max);
+    for (int y = 0; y < 8; y++) {
+        __m256 acc = zero;
+        for (int v = 0; v < 8; v++) acc = _mm256_add_ps(acc, _mm256_mul_ps(_mm256_broadcast_ss(t + 8 * y + v), tmp[v]));
+        __m256 s = _mm256_round_ps(_mm256_add_ps(_mm256_mul_ps(acc, sc), bias),
+                                   _MM_FROUND_TO_NEG_INF | _MM_FROUND_NO_EXC);
+        // max(s, 0) first: a NaN (which finite inputs cannot give) becomes 0,
+        // as in the scalar form.
+        s = _mm256_min_ps(_mm256_max_ps(s, zero), mx);
+        const __m256i w = _mm256_cvttps_epi32(s);
+        _mm_storeu_si128(reinterpret_cast<__m128i *>(out + 8 * y),
+                         _mm_packus_epi32(_mm256_castsi256_si128(w), _mm256_extracti128_si256(w, 1)));
+    }
+}
+
+// fdct_load_scalar, eight outputs at a time.
+void fdct_load_avx2(const uint16_t pix[64], float scale, float out[64]) {
+    const float *t = basis().t;
+    const __m256 zero = _mm256_setzero_ps(), sc = _mm256_set1_ps(scale), off = _mm256_set1_ps(256.0f);
+    alignas(32) float p[64];
+    for (int y = 0; y < 8; y++) {
+        const __m256i px = _mm256_cvtepu16_epi32(_mm_loadu_si128(reinterpret_cast<const __m128i *>(pix + 8 * y)));
+        _mm256_store_ps(p + 8 * y, _mm256_sub_ps(_mm256_mul_ps(_mm256_cvtepi32_ps(px), sc), off));
+    }
+    // Rows: tmp[y][u] = 0 + p[y][0] T[0][u] + ... + p[y][7] T[7][u].
+    __m256 tmp[8];
+    for (int y = 0; y < 8; y++) {
+        __m256 acc = zero;
+        for (int x = 0; x < 8; x++)
+            acc = _mm256_add_ps(acc, _mm256_mul_ps(_mm256_broadcast_ss(p + 8 * y + x), _mm256_loadu_ps(t + 8 * x)));
+        tmp[y] = acc;
+    }
+    // Columns: out[v][u] = 0 + T[0][v] tmp[0][u] + ... + T[7][v] tmp[7][u].
+    for (int v = 0; v < 8; v++) {
+        __m256 acc = zero;
+        for (int y = 0; y < 8; y++) acc = _mm256_add_ps(acc, _mm256_mul_ps(_mm256_broadcast_ss(t + 8 * y + v), tmp[y]));
+        _mm256_storeu_ps(out + 8 * v, acc);
+    }
+}
+
+// quantise_scalar, eight blocks of a scanned position at a time (n, the
+// component's block count, a multiple of 8; smaller components take the
+// scalar form).
+void quantise_avx2(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out, uint64_t *mask) {
+    if (n % 8 != 0) return quantise_scalar(f, n, inv, ac_rounding, out, mask);
+    for (size_t i = 0; i < n; i++) mask[i] = 0;
+    const __m256 zero = _mm256_setzero_ps(), sign = _mm256_set1_ps(-0.0f), big = _mm256_set1_ps(2147483648.0f);
+    const __m256i imax = _mm256_set1_epi32(INT32_MAX), izero = _mm256_setzero_si256();
+    for (size_t s = 0; s < 64; s++) {
+        const __m256 r = _mm256_set1_ps(s == 0 ? 0.5f : ac_rounding), iv = _mm256_set1_ps(inv[s]);
+        for (size_t b = 0; b < n; b += 8) {
+            const size_t i = n * s + b;
+            const __m256 x = _mm256_mul_ps(_mm256_loadu_ps(f + i), iv);
+            const __m256 fl = _mm256_round_ps(_mm256_add_ps(_mm256_andnot_ps(sign, x), r),
+                                              _MM_FROUND_TO_NEG_INF | _MM_FROUND_NO_EXC);
+            // Rust's saturating cast: NaN to 0, 2^31 and up to INT32_MAX.
+            __m256i m = _mm256_cvttps_epi32(fl);
+            m = _mm256_blendv_epi8(m, imax, _mm256_castps_si256(_mm256_cmp_ps(fl, big, _CMP_GE_OQ)));
+            m = _mm256_blendv_epi8(m, izero, _mm256_castps_si256(_mm256_cmp_ps(fl, fl, _CMP_UNORD_Q)));
+            const __m256i q = _mm256_blendv_epi8(m, _mm256_sub_epi32(izero, m),
+                                                 _mm256_castps_si256(_mm256_cmp_ps(x, zero, _CMP_LT_OQ)));
+            _mm256_storeu_si256(reinterpret_cast<__m256i *>(out + i), q);
+            const __m256i is_zero = _mm256_cmpeq_epi32(q, izero);
+            const uint32_t nz = ~(uint32_t)_mm256_movemask_ps(_mm256_castsi256_ps(is_zero)) & 0xFFu;
+            mask[i / 64] |= (uint64_t)nz << (i % 64);
+        }
+    }
+}
+
+void idct_put(const int32_t coef[64], const float scale[64], Output o, uint16_t out[64]) {
+    g_simd.load(std::memory_order_relaxed) ? idct_put_avx2(coef, scale, o, out) : idct_put_scalar(coef, scale, o, out);
+}
+void fdct_load(const uint16_t pix[64], float scale, float out[64]) {
+    g_simd.load(std::memory_order_relaxed) ? fdct_load_avx2(pix, scale, out) : fdct_load_scalar(pix, scale, out);
+}
+void quantise(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out, uint64_t *mask) {
+    if (g_simd.load(std::memory_order_relaxed))
+        quantise_avx2(f, n, inv, ac_rounding, out, mask);
+    else
+        quantise_scalar(f, n, inv, ac_rounding, out, mask);
 }
 
 // ---------------------------------------------------------------- pool
@@ -1840,6 +1972,7 @@ void ora_idct_put(const int32_t coef[64], const float scale[64], uint32_t bit_de
     idct_put(coef, scale, Output(bit_depth), out);
 }
 void ora_fdct_load(const uint16_t pix[64], float scale, float out[64]) { fdct_load(pix, scale, out); }
+void ora_set_simd(int on) { g_simd.store(on != 0); }
 void ora_quantise(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out, uint64_t *mask) {
     quantise(f, n, inv, ac_rounding, out, mask);
 }

@@ -89,6 +89,9 @@ void ora_basis(float basis[64]);
 /* Block kernels (src/dsp/scalar.rs). */
 void ora_idct_put(const int32_t coef[64], const float scale[64], uint32_t bit_depth, uint16_t out[64]);
 void ora_fdct_load(const uint16_t pix[64], float scale, float out[64]);
+/* Whether the dsp kernels (IDCT, FDCT, quantise) run their AVX2 forms (the
+ * default) or the scalar ones; both give the same results. */
+void ora_set_simd(int on);
 void ora_quantise(const float *f, size_t n, const float inv[64], float ac_rounding, int32_t *out,
                   uint64_t *mask);
 
